@@ -1,0 +1,445 @@
+"""Benchmark of the ZFP compress/decompress hot path on B200.
+
+Workload (one step): the 512^3 float64 field of the north-star's second
+configuration -- the smooth field sin(0.10x)cos(0.13y)sin(0.07z) + N(0,1e-3)
+scaled by 1e3, with 10% of its 4x4x4 blocks set to exactly zero and 1% of its
+values replaced by +-10^U(-30,30) spikes (seeded, synthetic) -- compressed and
+decompressed in fixed-accuracy 1e-6 and in fixed-precision 32 (variable-rate,
+so block offsets come from the device scan).  Rounding rotates per step over
+First/Last x tight_error off/on.  `value` is uncompressed GB coded per second:
+4 passes of 1 GiB per step (2 modes x compress + decompress) over the step's
+device time, inputs resident in HBM (1 GiB, larger than the 126 MB L2).
+
+`e2e` is the same step through the C ABI (zfp_compress / zfp_decompress)
+with host buffers in pinned memory: host->device copies of the field and the
+stream, and device->host copies of the stream and the decoded field, inside
+the timed region.
+
+Also reported (extra keys): fixed-rate 8 float32 512^3 compress/decompress
+GB/s and their roofline fractions, the north-star's headline target.
+
+--impl reference times the CPU restatement of zfp-rs (oracle/, the reference
+itself cannot be built here: no Rust toolchain) on the host cores, on bounded
+slabs of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+NX = NY = NZ = 512
+ROUNDINGS = [("first", False), ("first", True), ("last", False), ("last", True)]
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=512, help="cube side (default 512)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end measurement")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-fixed", action="store_true", help="skip the fixed-rate float32 measurement")
+    return ap.parse_args()
+
+
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def make_field_np(n, nz, seed=0):
+    """The first nz z-slices of the workload field on the host (numpy).
+
+    Same recipe as make_field, drawn from numpy's generator (a slab for the
+    CPU baseline; values differ from the device field but follow the same
+    distribution)."""
+    rng = np.random.default_rng(seed)
+    x = np.arange(n, dtype=np.float64)
+    z = np.arange(nz, dtype=np.float64)
+    f = (np.sin(0.10 * x)[None, None, :] * np.cos(0.13 * x)[None, :, None] * np.sin(0.07 * z)[:, None, None])
+    f = (f + rng.normal(0, 1e-3, size=(nz, n, n))) * 1e3
+    nb, nbz = n // 4, nz // 4
+    zero = rng.random((nbz, nb, nb)) < 0.10
+    f.reshape(nbz, 4, nb, 4, nb, 4)[zero[:, None, :, None, :, None].repeat(4, 1).repeat(4, 3).repeat(4, 5)] = 0.0
+    spikes = rng.random(f.shape) < 0.01
+    k = int(spikes.sum())
+    f[spikes] = rng.choice([-1.0, 1.0], size=k) * 10.0 ** rng.uniform(-30, 30, size=k)
+    return f
+
+
+def make_field(n, device, seed=0):
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    x = torch.arange(n, device=device, dtype=torch.float64)
+    f = (torch.sin(0.10 * x)[None, None, :] * torch.cos(0.13 * x)[None, :, None] * torch.sin(0.07 * x)[:, None, None])
+    f = (f + 1e-3 * torch.randn((n, n, n), generator=g, device=device, dtype=torch.float64)) * 1e3
+    nb = n // 4
+    zero = torch.rand((nb, nb, nb), generator=g, device=device) < 0.10
+    zmask = zero.repeat_interleave(4, 0).repeat_interleave(4, 1).repeat_interleave(4, 2)
+    f[zmask] = 0.0
+    spikes = torch.rand((n, n, n), generator=g, device=device) < 0.01
+    k = int(spikes.sum())
+    sign = torch.where(torch.rand(k, generator=g, device=device) < 0.5, -1.0, 1.0).to(torch.float64)
+    mag = 10.0 ** (torch.rand(k, generator=g, device=device, dtype=torch.float64) * 60 - 30)
+    f[spikes] = sign * mag
+    return f
+
+
+def smooth_f32(n, device, seed=0):
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    x = torch.arange(n, device=device, dtype=torch.float32)
+    f = (torch.sin(0.10 * x)[None, None, :] * torch.cos(0.13 * x)[None, :, None] * torch.sin(0.07 * x)[:, None, None])
+    return f + 1e-3 * torch.randn((n, n, n), generator=g, device=device, dtype=torch.float32)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index: int, path: Path):
+        self.path = path
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={q}", "--format=csv,noheader",
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                mx.append(float(parts[2].split()[0]))
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def max_over_ranks(pg, value, device):
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(n_side, threads, seconds_goal=15.0):
+    """The oracle (CPU restatement of zfp-rs) on slabs of the workload."""
+    from oracle import py_oracle as orc
+
+    slab_z = 32
+    field = make_field_np(n_side, slab_z)
+    cfgs = [orc.config(1, 16658, 64, -20, "first", False), orc.config(1, 16658, 32, -1074, "first", False)]
+    nbytes = 0
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        for cfg in cfgs:
+            stream, n = orc.compress(field, cfg, threads=threads)
+            out = np.zeros_like(field)
+            orc.decompress(stream, out, cfg, threads=threads)
+            nbytes += 2 * field.nbytes
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds_goal or reps >= 8:
+            break
+    return {"value": nbytes / el / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"{n_side}x{n_side}x{slab_z} float64 slab x {reps} reps, fixed-accuracy 1e-6 + fixed-precision 32, "
+                      f"compress (chunked threads) + decompress (variable-rate: serial, as the restatement has no "
+                      f"reader/worker pipeline)"}
+
+
+def run_reference(args):
+    ws, rank, local, pg = dist_setup(args)
+    if rank != 0:
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        pass
+    vals = []
+    samples = []
+    for _ in range(args.steps):
+        cb = cpu_baseline(args.size, threads, seconds_goal=4.0)
+        vals.append(cb["value"])
+        samples.append(cb)
+    v = float(np.mean(vals))
+    line = {"metric": "compress/decompress GB/s on 1 B200 (bit-exact); batched p50/p99 ms",
+            "impl": "reference", "value": v, "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.size}^3 float64, fixed-accuracy 1e-6 + fixed-precision 32, "
+                                   "rounding First/Last x tight", "sampled": samples[0]["sample"]},
+            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
+                             "sample": samples[0]["sample"]},
+            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    ws, rank, local, pg = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from tests import zfpb
+
+    Z = zfpb.load()
+    L = Z.lib()
+    n = args.size
+    field = make_field(n, dev, seed=rank)
+    nbytes = field.numel() * 8
+    cfgs = {
+        "accuracy_1e-6": Z.ZfpConfig.fixed_accuracy(1e-6),
+        "precision_32": Z.ZfpConfig.fixed_precision(32),
+    }
+    cap = max(Z.maximum_size(field.shape, np.float64, c) for c in cfgs.values())
+    stream_buf = torch.empty((cap + 7) // 8, dtype=torch.int64, device=dev)
+    nblocks = (n // 4) ** 3
+    offsets = torch.empty(nblocks + 1, dtype=torch.int64, device=dev)
+    out = torch.empty_like(field)
+    cs = torch.cuda.current_stream(dev)
+
+    stream_bytes = {}
+
+    def step(i):
+        rnd, tight = ROUNDINGS[i % len(ROUNDINGS)]
+        for name, cfg in cfgs.items():
+            c = cfg.with_rounding(rnd, tight)
+            nb = Z.compress_device(field, c, out=stream_buf, offsets=offsets)
+            stream_bytes[(name, i % len(ROUNDINGS))] = nb
+            Z.decompress_device(stream_buf, nb, out, c, offsets=offsets)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize(dev)
+    if pg is not None:
+        pg.barrier()
+    clocks = ClockSampler(local, ROOT / "gpurun_out" / f"clocks_rank{rank}.csv") if rank == 0 else None
+    Z.timing_enable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(cs)
+    for i in range(args.steps):
+        step(i)
+    e1.record(cs)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    ktimes = Z.timing_read()
+    Z.timing_enable(False)
+    clock_info = clocks.stop() if clocks else None
+    ms = max_over_ranks(pg, ms, dev)
+    if pg is not None:
+        pg.barrier()
+    ms_per_step = ms / args.steps
+    total_bytes = ws * args.steps * 4 * nbytes
+    value = total_bytes / (ms / 1e3) / 1e9
+
+    # Roofline of the dominant kernel: algorithmic bytes (field + stream) per
+    # launch over its average duration, from the event timers above.
+    mean_stream = float(np.mean(list(stream_bytes.values())))
+    kinds = {k: v for k, v in ktimes.items() if v[1] > 0}
+    dom = max(kinds, key=lambda k: kinds[k][0])
+    dom_ms, dom_n = kinds[dom]
+    algo = nbytes + mean_stream if dom in ("encode_var", "decode_var", "encode_fixed", "decode_fixed") else None
+    peak, peak_kind = hbm_peak()
+    roof = None
+    if algo is not None:
+        achieved = algo / (dom_ms / dom_n / 1e3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic_of(dom),
+                "algorithmic_bytes_per_launch": algo, "avg_launch_ms": dom_ms / dom_n, "launches": dom_n}
+    launches = int(sum(v[1] for v in ktimes.values()) + 2 * ktimes["scan"][1])  # a scan is 3 kernels
+
+    # End to end through the C ABI with pinned host buffers.
+    e2e = None if args.no_e2e else e2e_measure(Z, L, field, cfgs, cap, args, dev)
+
+    # Fixed-rate 8 float32 (north-star headline target), device resident.
+    fr = None if args.no_fixed else fixed_rate_measure(Z, n, dev, args, peak)
+
+    if rank == 0:
+        line = {
+            "metric": "compress/decompress GB/s on 1 B200 (bit-exact); batched p50/p99 ms",
+            "value": value, "unit": "GB/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{n}^3 float64 smooth x1e3 + 10% zero blocks + 1% spikes; fixed-accuracy 1e-6 and "
+                                   f"fixed-precision 32, rounding First/Last x tight rotating per step",
+                       "passes_per_step": "2 modes x (compress + decompress) of 1 field",
+                       "l2": "inputs (1 GiB) larger than L2", "parallelism": f"replicas x{ws}",
+                       "mean_stream_bytes": mean_stream},
+            "roofline": roof,
+            "kernel_ms": {k: {"total_ms": v[0], "launches": v[1]} for k, v in kinds.items()},
+            "gpu_launches": launches,
+            "e2e": e2e,
+            "fixed_rate_f32": fr,
+            "clocks": clock_info,
+        }
+        if ws == 1 and not args.no_cpu:
+            line["cpu_baseline"] = cpu_baseline(n, os.cpu_count() or 1)
+        print(json.dumps(line))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def traffic_of(kind):
+    """DRAM bytes per launch of a kernel kind from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "traffic.json"
+    try:
+        return json.loads(p.read_text()).get(kind)
+    except Exception:
+        return None
+
+
+def e2e_measure(Z, L, field, cfgs, cap, args, dev):
+    import torch
+
+    host_field = torch.empty(field.shape, dtype=torch.float64, pin_memory=True)
+    host_field.copy_(field.cpu())
+    host_out = torch.empty_like(host_field).pin_memory()
+    host_stream = torch.empty((cap + 7) // 8 + 1, dtype=torch.int64, pin_memory=True)
+    fnp = host_field.numpy()
+    onp = host_out.numpy()
+    snp = host_stream.numpy()
+    bs = L.stream_open(snp.ctypes.data, snp.nbytes)
+    zs = L.zfp_stream_open(bs)
+    f_in = Z.field_of(fnp)
+    f_out = Z.field_of(onp)
+    h2d = d2h = 0
+
+    def step(i):
+        nonlocal h2d, d2h
+        rnd, tight = ROUNDINGS[i % len(ROUNDINGS)]
+        for cfg in cfgs.values():
+            c = cfg.with_rounding(rnd, tight)
+            L.zfp_stream_set_params(zs, c.min_bits, c.max_bits, c.max_prec, c.min_exp)
+            L.zfp_stream_set_rounding(zs, c.rounding_code, int(c.tight_error))
+            L.zfp_stream_rewind(zs)
+            nb = L.zfp_compress(zs, C.byref(f_in))
+            assert nb > 0, L.zfpb_last_error()
+            L.zfp_stream_rewind(zs)
+            assert L.zfp_decompress(zs, C.byref(f_out)) == nb
+            h2d += fnp.nbytes + nb
+            d2h += nb + onp.nbytes
+
+    for i in range(args.warmup):
+        step(i)
+    h2d = d2h = 0
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        step(i)
+    torch.cuda.synchronize(dev)
+    el = time.perf_counter() - t0
+    L.zfp_stream_close(zs)
+    L.stream_close(bs)
+    total = args.steps * 4 * fnp.nbytes
+    return {"value": total / el / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d // args.steps,
+            "d2h_bytes_per_step": d2h // args.steps, "ms_per_step": el * 1e3 / args.steps,
+            "path": "zfp_compress/zfp_decompress (include/zfp.h) on pinned host buffers"}
+
+
+def fixed_rate_measure(Z, n, dev, args, peak):
+    import torch
+
+    x = smooth_f32(n, dev)
+    cfg = Z.ZfpConfig.fixed_rate(8, np.float32, 3)
+    cap = Z.maximum_size(x.shape, np.float32, cfg)
+    sb = torch.empty((cap + 7) // 8, dtype=torch.int64, device=dev)
+    y = torch.empty_like(x)
+    nb = 0
+    for _ in range(max(3, args.warmup)):
+        nb = Z.compress_device(x, cfg, out=sb)
+        Z.decompress_device(sb, nb, y, cfg)
+    torch.cuda.synchronize(dev)
+    Z.timing_enable(True)
+    reps = max(5, args.steps)
+    for _ in range(reps):
+        Z.compress_device(x, cfg, out=sb)
+        Z.decompress_device(sb, nb, y, cfg)
+    torch.cuda.synchronize(dev)
+    kt = Z.timing_read()
+    Z.timing_enable(False)
+    fb = x.numel() * 4
+    res = {"workload": f"{n}^3 float32 smooth + N(0,1e-3), fixed-rate 8", "stream_bytes": nb}
+    for kind, key in (("encode_fixed", "compress"), ("decode_fixed", "decompress")):
+        ms, cnt = kt[kind]
+        if cnt:
+            t = ms / cnt / 1e3
+            res[f"{key}_gbs"] = fb / t / 1e9
+            res[f"{key}_roofline_frac"] = (fb + nb) / t / 1e9 / peak
+            res[f"{key}_ms"] = t * 1e3
+    return res
+
+
+if __name__ == "__main__":
+    main()

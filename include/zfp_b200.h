@@ -1,0 +1,70 @@
+/*
+ * zfp_b200.h -- extensions of libzfp_b200.so beyond the zfp.h ABI.
+ *
+ * None of these replaces a zfp.h function; each gives C callers something
+ * zfp-rs offers only through its Rust API, or a device-memory entry point.
+ */
+#ifndef ZFP_B200_EXT_H
+#define ZFP_B200_EXT_H
+
+#include "zfp.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Coefficient rounding of a stream opened with zfp_stream_open, as zfp-rs's
+ * per-call ZfpRounding (src/config.rs:115-138), which zfp-rs-ffi instead fixes
+ * at build time (zfp-rs-ffi/src/stream.rs:12-16).  rounding: ZFP_ROUND_NEVER,
+ * ZFP_ROUND_FIRST or ZFP_ROUND_LAST.  Returns zfp_false for an invalid value.
+ * New streams round ZFP_ROUND_NEVER without tight error. */
+zfp_bool zfp_stream_set_rounding(zfp_stream* stream, int rounding, zfp_bool tight_error);
+int zfp_stream_rounding(const zfp_stream* stream, zfp_bool* tight_error);
+
+/* Status of the last failed call on this thread: 0 none, 1 buffer too small,
+ * 2 truncated stream, 3 CUDA error, 4 invalid arguments. */
+int zfpb_last_error(void);
+
+/* A field and codec parameters in one plain struct for the device API. */
+typedef struct zfpb_desc {
+  zfp_type type;
+  size_t nx, ny, nz, nw;       /* zero past the dimensionality */
+  ptrdiff_t sx, sy, sz, sw;    /* element strides, 0 = natural */
+  uint minbits, maxbits, maxprec;
+  int32_t minexp;
+  int rounding;                /* ZFP_ROUND_NEVER / _FIRST / _LAST */
+  zfp_bool tight_error;
+} zfpb_desc;
+
+/* Compress a device-resident field (d_field points at element [0,0,0,0]) into
+ * the device buffer d_stream of `capacity` bytes (8-byte aligned), starting at
+ * bit 0 with no header.  d_block_offsets, if not NULL, receives nblocks + 1
+ * bit offsets: where each block starts and where the last one ends.
+ * cuda_stream is a cudaStream_t (NULL: the default stream).  Returns the
+ * stream size in bytes, or 0 on failure; the call returns once the stream is
+ * complete. */
+size_t zfpb_compress_device(const zfpb_desc* desc, const void* d_field, void* d_stream, size_t capacity,
+                            uint64_t* d_block_offsets, void* cuda_stream);
+
+/* Decompress `bytes` bytes of a headerless stream at d_stream into the
+ * device-resident field d_field.  d_block_offsets (optional) are candidate
+ * block offsets, e.g. from zfpb_compress_device; they are used only if they
+ * match the stream, else the offsets are recomputed from the stream.
+ * Returns the bytes consumed, or 0 on failure (e.g. a truncated stream). */
+size_t zfpb_decompress_device(const zfpb_desc* desc, const void* d_stream, size_t bytes, void* d_field,
+                              const uint64_t* d_block_offsets, void* cuda_stream);
+
+/* Per-kernel timing for profiling: when enabled, every kernel launch of the
+ * library is bracketed by CUDA events on its stream.  zfpb_timing_enable
+ * clears the totals.  zfpb_timing_read fills, per kernel kind, the summed
+ * milliseconds and the launch count, and returns the number of kinds:
+ * 0 encode_fixed, 1 encode_var, 2 scan, 3 pack, 4 decode_fixed,
+ * 5 decode_var, 6 walk, 7 claim, 8 offsets. */
+void zfpb_timing_enable(int on);
+int zfpb_timing_read(double* ms, unsigned long long* counts, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZFP_B200_EXT_H */

@@ -1,0 +1,1088 @@
+// Device-side ZFP block codec for sm_100a: one thread codes one 4^d block.
+//
+// The stream format and every arithmetic step follow zfp-rs 1.0.1:
+//   lifting transforms        src/codec/transform.rs:74-233
+//   cast, rounding, negabinary src/codec/encode/core.rs:53-423
+//   embedded bit-plane coder  src/codec/bitplane.rs:509-790
+//   block coders              src/codec/encode/{float,integer,reversible}.rs,
+//                             src/codec/decode/{core,reversible}.rs
+// The implementation is GPU-shaped: coefficients live in registers (all
+// indices compile-time after unrolling), bit planes are produced by an
+// in-register bit-matrix transpose and kept in a per-thread slice of shared
+// memory for the data-dependent plane loop, and stream words are assembled in
+// a 64-bit register before a single store.
+#pragma once
+
+#include <cstdint>
+#include <type_traits>
+#include <utility>
+
+#include "zfpb_engine.h"
+
+namespace zfpb {
+
+typedef unsigned long long u64;
+typedef unsigned int u32;
+typedef long long i64;
+
+#define ZFPB_DEV __device__ __forceinline__
+
+// ---------------------------------------------------------------------------
+// Scalar traits (zfp-rs src/types.rs:327-344, encode/core.rs:309-325)
+// ---------------------------------------------------------------------------
+
+template <class T> struct Traits;
+template <> struct Traits<float> {
+  typedef int I; typedef u32 U;
+  static constexpr int EBITS = 8, EBIAS = 127, PREC = 32, PBITS = 5, MIN_CAST_EMAX = -97;
+  static constexpr bool FLOAT = true;
+};
+template <> struct Traits<double> {
+  typedef i64 I; typedef u64 U;
+  static constexpr int EBITS = 11, EBIAS = 1023, PREC = 64, PBITS = 6, MIN_CAST_EMAX = -961;
+  static constexpr bool FLOAT = true;
+};
+template <> struct Traits<int> {
+  typedef int I; typedef u32 U;
+  static constexpr int EBITS = 0, EBIAS = 0, PREC = 32, PBITS = 5, MIN_CAST_EMAX = 0;
+  static constexpr bool FLOAT = false;
+};
+template <> struct Traits<i64> {
+  typedef i64 I; typedef u64 U;
+  static constexpr int EBITS = 0, EBIAS = 0, PREC = 64, PBITS = 6, MIN_CAST_EMAX = 0;
+  static constexpr bool FLOAT = false;
+};
+
+// Parameters of one compress/decompress call (zfp-rs src/config.rs:163-174):
+// minbits, maxbits, maxprec, minexp, rounding (0 never, 1 first, 2 last), tight.
+typedef CodecParams Codec;
+
+static constexpr int ZFP_MIN_EXP = -1074;
+
+// ---------------------------------------------------------------------------
+// Coefficient order (zfp-rs src/codec/encode/core.rs:12-39).  These tables
+// are the stream format; they are evaluated at compile time after unrolling.
+// ---------------------------------------------------------------------------
+
+__host__ __device__ constexpr int perm2(int i) {
+  constexpr unsigned char t[16] = {0, 1, 4, 5, 2, 8, 6, 9, 3, 12, 10, 7, 13, 11, 14, 15};
+  return t[i];
+}
+__host__ __device__ constexpr int perm3(int i) {
+  constexpr unsigned char t[64] = {
+      0,  1,  4,  16, 20, 17, 5,  2,  8,  32, 21, 6,  18, 24, 9,  33, 36, 3,  12, 48, 22, 25,
+      37, 40, 34, 10, 7,  19, 28, 13, 49, 52, 41, 38, 26, 23, 29, 53, 11, 35, 44, 14, 50, 56,
+      42, 27, 39, 45, 30, 54, 57, 60, 51, 15, 43, 46, 58, 61, 55, 31, 62, 59, 47, 63};
+  return t[i];
+}
+__device__ const unsigned char kPerm4[256] = {
+    0,   1,   4,   16,  64,  5,   80,  17,  68,  65,  20,  2,   8,   32,  128, 84,  81,  69,  21,
+    6,   18,  66,  24,  72,  9,   96,  33,  36,  129, 132, 144, 3,   12,  48,  192, 85,  82,  70,
+    22,  73,  25,  88,  37,  100, 97,  148, 145, 133, 10,  160, 34,  136, 130, 40,  7,   19,  67,
+    28,  76,  13,  112, 49,  52,  193, 196, 208, 86,  89,  101, 149, 161, 137, 41,  134, 38,  164,
+    26,  152, 146, 104, 98,  74,  83,  71,  23,  77,  29,  92,  53,  116, 113, 212, 209, 197, 11,
+    35,  131, 44,  140, 14,  176, 50,  56,  194, 200, 224, 90,  165, 102, 153, 150, 105, 168, 162,
+    138, 42,  87,  93,  117, 213, 27,  75,  99,  39,  135, 147, 108, 45,  141, 156, 30,  78,  177,
+    180, 54,  114, 120, 57,  198, 210, 216, 201, 225, 228, 15,  240, 51,  204, 195, 60,  169, 166,
+    154, 106, 91,  103, 151, 109, 157, 94,  181, 118, 121, 214, 217, 229, 163, 139, 43,  142, 46,
+    172, 58,  184, 178, 232, 226, 202, 241, 205, 61,  199, 55,  244, 31,  220, 211, 124, 115, 79,
+    170, 167, 155, 107, 158, 110, 173, 122, 185, 182, 233, 230, 218, 95,  245, 119, 221, 215, 125,
+    242, 206, 62,  203, 59,  248, 47,  236, 227, 188, 179, 143, 171, 174, 186, 234, 246, 222, 126,
+    219, 123, 249, 111, 237, 231, 189, 183, 159, 252, 243, 207, 63,  175, 250, 187, 238, 235, 190,
+    253, 247, 223, 127, 254, 251, 239, 191, 255};
+
+template <class I> ZFPB_DEV typename Traits<I>::U int2uint(I x);
+ZFPB_DEV int uint2int(u32 x);
+ZFPB_DEV i64 uint2int(u64 x);
+
+template <int N> ZFPB_DEV int perm_at(int i) {
+  if constexpr (N == 4) return i;
+  else if constexpr (N == 16) return perm2(i);
+  else if constexpr (N == 64) return perm3(i);
+  else return kPerm4[i];
+}
+
+// Compile-time loop: f(std::integral_constant<int, i>) for i in [0, N), so
+// that table lookups indexed by i are constant expressions.
+template <class F, int... Is>
+ZFPB_DEV void static_for_impl(F&& f, std::integer_sequence<int, Is...>) {
+  (f(std::integral_constant<int, Is>{}), ...);
+}
+template <int N, class F> ZFPB_DEV void static_for(F&& f) {
+  static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+// u[i] = int2uint(b[perm[i]]) (encode/core.rs:98-109) and its inverse
+// b[perm[i]] = uint2int(u[i]) (decode/core.rs:40-51).
+template <int N, class I, class U> ZFPB_DEV void fwd_order(U* u, const I* b) {
+  if constexpr (N == 256) {
+    for (int i = 0; i < N; i++) u[i] = int2uint(b[kPerm4[i]]);
+  } else {
+    static_for<N>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      constexpr int p = N == 4 ? i : N == 16 ? perm2(i) : perm3(i);
+      u[i] = int2uint(b[p]);
+    });
+  }
+}
+template <int N, class I, class U> ZFPB_DEV void inv_order(const U* u, I* b) {
+  if constexpr (N == 256) {
+    for (int i = 0; i < N; i++) b[kPerm4[i]] = uint2int(u[i]);
+  } else {
+    static_for<N>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      constexpr int p = N == 4 ? i : N == 16 ? perm2(i) : perm3(i);
+      b[p] = uint2int(u[i]);
+    });
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Exact powers of two by exponent-field construction (no libm): 2^n rounded
+// to the format, i.e. subnormal below the normal range, 0 below half the
+// smallest subnormal, infinity above the largest finite exponent.
+// ---------------------------------------------------------------------------
+
+ZFPB_DEV float pow2f(int n) {
+  if (n > 127) return __int_as_float(0x7f800000);
+  if (n >= -126) return __int_as_float((n + 127) << 23);
+  if (n >= -149) return __int_as_float(1 << (n + 149));
+  return 0.0f;
+}
+ZFPB_DEV double pow2d(int n) {
+  if (n > 1023) return __longlong_as_double(0x7ff0000000000000ll);
+  if (n >= -1022) return __longlong_as_double((i64)(n + 1023) << 52);
+  if (n >= -1074) return __longlong_as_double(1ll << (n + 1074));
+  return 0.0;
+}
+template <class T> ZFPB_DEV T pow2(int n);
+template <> ZFPB_DEV float pow2<float>(int n) { return pow2f(n); }
+template <> ZFPB_DEV double pow2<double>(int n) { return pow2d(n); }
+
+ZFPB_DEV u32 bits_of(float f) { return (u32)__float_as_int(f); }
+ZFPB_DEV u64 bits_of(double f) { return (u64)__double_as_longlong(f); }
+ZFPB_DEV float float_of(u32 u) { return __int_as_float((int)u); }
+ZFPB_DEV double float_of(u64 u) { return __longlong_as_double((i64)u); }
+
+// x86-64 truncation (zfp-rs encode/core.rs:385-423): out of range or NaN gives
+// the minimum integer.  Explicit round-toward-zero conversions after the range
+// check, so the result does not depend on the hardware's saturation rule.
+ZFPB_DEV int trunc_i(float v) {
+  return (v >= -2147483648.0f && v < 2147483648.0f) ? __float2int_rz(v) : (int)0x80000000;
+}
+ZFPB_DEV i64 trunc_i(double v) {
+  return (v >= -9223372036854775808.0 && v < 9223372036854775808.0) ? __double2ll_rz(v)
+                                                                       : (i64)0x8000000000000000ll;
+}
+// Round-to-nearest integer -> float conversions (decode/core.rs:162-175).
+ZFPB_DEV float to_float(int i) { return __int2float_rn(i); }
+ZFPB_DEV double to_float(i64 i) { return __ll2double_rn(i); }
+ZFPB_DEV float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+ZFPB_DEV double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
+// ---------------------------------------------------------------------------
+// Lifting transforms with two's-complement wraparound (transform.rs:74-142)
+// ---------------------------------------------------------------------------
+
+template <class I> ZFPB_DEV I wadd(I a, I b) {
+  typedef typename Traits<I>::U U;
+  return (I)((U)a + (U)b);
+}
+template <class I> ZFPB_DEV I wsub(I a, I b) {
+  typedef typename Traits<I>::U U;
+  return (I)((U)a - (U)b);
+}
+
+template <class I> ZFPB_DEV void fwd_lift(I& x, I& y, I& z, I& w) {
+  x = wadd(x, w) >> 1; w = wsub(w, x);
+  z = wadd(z, y) >> 1; y = wsub(y, z);
+  x = wadd(x, z) >> 1; z = wsub(z, x);
+  w = wadd(w, y) >> 1; y = wsub(y, w);
+  w = wadd(w, (I)(y >> 1));
+  y = wsub(y, (I)(w >> 1));
+}
+template <class I> ZFPB_DEV void inv_lift(I& x, I& y, I& z, I& w) {
+  y = wadd(y, (I)(w >> 1));
+  w = wsub(w, (I)(y >> 1));
+  y = wadd(y, w);
+  w = wsub(w, wsub(y, w));
+  z = wadd(z, x);
+  x = wsub(x, wsub(z, x));
+  y = wadd(y, z);
+  z = wsub(z, wsub(y, z));
+  w = wadd(w, x);
+  x = wsub(x, wsub(w, x));
+}
+template <class I> ZFPB_DEV void rev_fwd_lift(I& x, I& y, I& z, I& w) {
+  w = wsub(w, z); z = wsub(z, y); y = wsub(y, x);
+  w = wsub(w, z); z = wsub(z, y); w = wsub(w, z);
+}
+template <class I> ZFPB_DEV void rev_inv_lift(I& x, I& y, I& z, I& w) {
+  w = wadd(w, z); z = wadd(z, y); w = wadd(w, z);
+  y = wadd(y, x); z = wadd(z, y); w = wadd(w, z);
+}
+
+// Lift every line of stride S in a block of N values (transform.rs:151-170).
+template <class I, int N, int S, int KIND> ZFPB_DEV void lift_axis(I* p) {
+#pragma unroll
+  for (int g = 0; g < N; g += 4 * S) {
+#pragma unroll
+    for (int i = g; i < g + S; i++) {
+      if constexpr (KIND == 0) fwd_lift(p[i], p[i + S], p[i + 2 * S], p[i + 3 * S]);
+      else if constexpr (KIND == 1) inv_lift(p[i], p[i + S], p[i + 2 * S], p[i + 3 * S]);
+      else if constexpr (KIND == 2) rev_fwd_lift(p[i], p[i + S], p[i + 2 * S], p[i + 3 * S]);
+      else rev_inv_lift(p[i], p[i + S], p[i + 2 * S], p[i + 3 * S]);
+    }
+  }
+}
+// Forward: axes x, y, z, w; inverse: w, z, y, x (transform.rs:174-233).
+template <class I, int N, int KIND> ZFPB_DEV void fwd_axes(I* p) {
+  lift_axis<I, N, 1, KIND>(p);
+  if constexpr (N >= 16) lift_axis<I, N, 4, KIND>(p);
+  if constexpr (N >= 64) lift_axis<I, N, 16, KIND>(p);
+  if constexpr (N >= 256) lift_axis<I, N, 64, KIND>(p);
+}
+template <class I, int N, int KIND> ZFPB_DEV void inv_axes(I* p) {
+  if constexpr (N >= 256) lift_axis<I, N, 64, KIND>(p);
+  if constexpr (N >= 64) lift_axis<I, N, 16, KIND>(p);
+  if constexpr (N >= 16) lift_axis<I, N, 4, KIND>(p);
+  lift_axis<I, N, 1, KIND>(p);
+}
+
+// ---------------------------------------------------------------------------
+// Negabinary and rounding (encode/core.rs:53-91, decode/core.rs:21-82)
+// ---------------------------------------------------------------------------
+
+template <class U> ZFPB_DEV U nbmask() { return (U)0xaaaaaaaaaaaaaaaaull; }
+
+template <class I> ZFPB_DEV typename Traits<I>::U int2uint(I x) {
+  typedef typename Traits<I>::U U;
+  return (U)((U)x + nbmask<U>()) ^ nbmask<U>();
+}
+ZFPB_DEV int uint2int(u32 x) { return (int)((x ^ 0xaaaaaaaau) - 0xaaaaaaaau); }
+ZFPB_DEV i64 uint2int(u64 x) { return (i64)((x ^ 0xaaaaaaaaaaaaaaaaull) - 0xaaaaaaaaaaaaaaaaull); }
+
+template <class I, int N> ZFPB_DEV void fwd_round(I* b, u32 maxprec) {
+  typedef typename Traits<I>::U U;
+  constexpr u32 B = sizeof(U) * 8;
+  if (maxprec < B) {
+    I bias = (I)((U)(nbmask<U>() >> 2) >> maxprec);
+    if (!(maxprec & 1)) bias = wsub((I)0, bias);
+#pragma unroll
+    for (int i = 0; i < N; i++) b[i] = wadd(b[i], bias);
+  }
+}
+
+template <class U, int N> ZFPB_DEV void inv_round(U* d, u32 m, u32 prec) {
+  constexpr u32 B = sizeof(U) * 8;
+  if (prec < B - 1) {
+    U hi = (U)(nbmask<U>() >> 2) >> prec;
+    U lo = (U)(nbmask<U>() >> 1) >> prec;
+#pragma unroll
+    for (int i = 0; i < N; i++) d[i] += ((u32)i < m) ? hi : lo;
+  }
+}
+
+ZFPB_DEV bool with_maxbits(u32 maxbits, u32 maxprec, u32 size) {
+  return ((u64)maxprec + 1) * (u64)size > (u64)maxbits + 1;
+}
+
+// encode/core.rs:231-244
+ZFPB_DEV u32 precision_f(int maxexp, u32 maxprec, int minexp, u32 dims, bool tight) {
+  i64 raw = (i64)maxexp - (i64)minexp + 2 * (i64)dims + (tight ? 1 : 2);
+  raw = raw < 0 ? 0 : raw;
+  raw = raw > (i64)maxprec ? (i64)maxprec : raw;
+  return (u32)raw;
+}
+
+ZFPB_DEV u32 sat_sub(u32 a, u32 b) { return a > b ? a - b : 0u; }
+
+// ---------------------------------------------------------------------------
+// Block-floating-point (encode/core.rs:251-380, decode/core.rs:162-175)
+// ---------------------------------------------------------------------------
+
+// frexp exponent of the largest |x|, NaNs skipped: fmax ignores a NaN operand.
+template <class T, int N> ZFPB_DEV int exponent_block(const T* d) {
+  T m = 0;
+#pragma unroll
+  for (int i = 0; i < N; i++) m = fmax(m, fabs(d[i]));
+  auto b = bits_of(m);
+  if constexpr (sizeof(T) == 4) {
+    u32 e = b >> 23;
+    return b == 0 ? -127 : (e == 0xff ? 0 : (int)e - 126);
+  } else {
+    u32 e = (u32)(b >> 52);
+    return b == 0 ? -1023 : (e == 0x7ff ? 0 : (int)e - 1022);
+  }
+}
+
+template <class T, int N>
+ZFPB_DEV void fwd_cast(typename Traits<T>::I* ib, const T* fb, int emax) {
+  constexpr int ip = Traits<T>::PREC;
+  if (emax < Traits<T>::MIN_CAST_EMAX) {
+    // Two exact steps for blocks whose one-step scale overflows.
+    T s = pow2<T>(ip - 2 - 64 - emax);
+    T two64 = pow2<T>(64);
+#pragma unroll
+    for (int i = 0; i < N; i++) ib[i] = trunc_i(mul_rn(mul_rn(fb[i], two64), s));
+  } else {
+    T s = pow2<T>(ip - 2 - emax);
+#pragma unroll
+    for (int i = 0; i < N; i++) ib[i] = trunc_i(mul_rn(s, fb[i]));
+  }
+}
+
+template <class T, int N>
+ZFPB_DEV void inv_cast(const typename Traits<T>::I* ib, T* fb, int emax) {
+  constexpr int ip = Traits<T>::PREC;
+  T s = pow2<T>(emax - (ip - 2));
+#pragma unroll
+  for (int i = 0; i < N; i++) fb[i] = mul_rn(s, to_float(ib[i]));
+}
+
+// ---------------------------------------------------------------------------
+// Bit-matrix transposes (Hacker's Delight 7-3, as bitplane.rs:75-92): row i
+// is a[i], column c is bit c.
+// ---------------------------------------------------------------------------
+
+template <class W, int J> ZFPB_DEV void transpose_stage(W* a, int R) {
+  W m;
+  if constexpr (J == 32) m = (W)0x00000000ffffffffull;
+  else if constexpr (J == 16) m = (W)0x0000ffff0000ffffull;
+  else if constexpr (J == 8) m = (W)0x00ff00ff00ff00ffull;
+  else if constexpr (J == 4) m = (W)0x0f0f0f0f0f0f0f0full;
+  else if constexpr (J == 2) m = (W)0x3333333333333333ull;
+  else m = (W)0x5555555555555555ull;
+#pragma unroll
+  for (int k = 0; k < 64; k += 2 * J) {
+    if (k >= R) break;
+#pragma unroll
+    for (int i = k; i < k + J; i++) {
+      W t = ((a[i] >> J) ^ a[i + J]) & m;
+      a[i] ^= t << J;
+      a[i + J] ^= t;
+    }
+  }
+}
+
+// Stages are separate instantiations so every index is a compile-time
+// constant and the matrix stays in registers.
+template <class W, int R> ZFPB_DEV void transpose(W* a) {
+  if constexpr (R >= 64) transpose_stage<W, 32>(a, R);
+  transpose_stage<W, 16>(a, R);
+  transpose_stage<W, 8>(a, R);
+  transpose_stage<W, 4>(a, R);
+  transpose_stage<W, 2>(a, R);
+  transpose_stage<W, 1>(a, R);
+}
+
+// Per-thread plane storage in shared memory: plane k, word c of thread t is
+// at base[(k * W + c) * stride + t]; consecutive threads hit consecutive
+// words, so a warp's accesses are bank-conflict free.
+struct PlaneStore {
+  u64* base;
+  int stride;
+  ZFPB_DEV u64& at(int k, int c, int W) const { return base[(size_t)(k * W + c) * stride]; }
+};
+
+// Coefficients -> bit planes k = 0..PREC-1 (plane k, bit i = bit k of u[i]).
+template <class U, int N> ZFPB_DEV void store_planes(const U* u, PlaneStore ps) {
+  constexpr int P = sizeof(U) * 8;
+  constexpr int W = N <= 64 ? 1 : N / 64;
+  if constexpr (N == 4) {
+#pragma unroll
+    for (int k = 0; k < P; k++) {
+      u64 x = 0;
+#pragma unroll
+      for (int i = 0; i < 4; i++) x |= (u64)((u[i] >> k) & 1) << i;
+      ps.at(k, 0, 1) = x;
+    }
+  } else if constexpr (sizeof(U) == 4 && N == 16) {
+    u32 a[32];
+#pragma unroll
+    for (int i = 0; i < 32; i++) a[i] = i < 16 ? u[i] : 0u;
+    transpose<u32, 32>(a);
+#pragma unroll
+    for (int k = 0; k < 32; k++) ps.at(k, 0, 1) = a[k];
+  } else if constexpr (sizeof(U) == 4) {
+    // 64 coefficients per chunk, as two 32x32 transposes.
+#pragma unroll
+    for (int c = 0; c < W; c++) {
+      u32 lo[32], hi[32];
+#pragma unroll
+      for (int i = 0; i < 32; i++) {
+        lo[i] = u[64 * c + i];
+        hi[i] = u[64 * c + 32 + i];
+      }
+      transpose<u32, 32>(lo);
+      transpose<u32, 32>(hi);
+#pragma unroll
+      for (int k = 0; k < 32; k++) ps.at(k, c, W) = (u64)lo[k] | ((u64)hi[k] << 32);
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < W; c++) {
+      u64 a[64];
+#pragma unroll
+      for (int i = 0; i < 64; i++) a[i] = (64 * c + i) < N ? (u64)u[64 * c + i] : 0ull;
+      transpose<u64, 64>(a);
+#pragma unroll
+      for (int k = 0; k < 64; k++) ps.at(k, c, W) = a[k];
+    }
+  }
+}
+
+// Bit planes -> coefficients; planes outside [lo, hi] are zero.
+template <class U, int N> ZFPB_DEV void load_planes(U* u, PlaneStore ps, int lo, int hi) {
+  constexpr int P = sizeof(U) * 8;
+  constexpr int W = N <= 64 ? 1 : N / 64;
+  if constexpr (N == 4) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) u[i] = 0;
+#pragma unroll
+    for (int k = 0; k < P; k++) {
+      u64 x = (k >= lo && k <= hi) ? ps.at(k, 0, 1) : 0ull;
+#pragma unroll
+      for (int i = 0; i < 4; i++) u[i] |= (U)((x >> i) & 1) << k;
+    }
+  } else if constexpr (sizeof(U) == 4 && N == 16) {
+    u32 a[32];
+#pragma unroll
+    for (int k = 0; k < 32; k++) a[k] = (k >= lo && k <= hi) ? (u32)ps.at(k, 0, 1) : 0u;
+    transpose<u32, 32>(a);
+#pragma unroll
+    for (int i = 0; i < 16; i++) u[i] = a[i];
+  } else if constexpr (sizeof(U) == 4) {
+#pragma unroll
+    for (int c = 0; c < W; c++) {
+      u32 a[32], b[32];
+#pragma unroll
+      for (int k = 0; k < 32; k++) {
+        u64 x = (k >= lo && k <= hi) ? ps.at(k, c, W) : 0ull;
+        a[k] = (u32)x;
+        b[k] = (u32)(x >> 32);
+      }
+      transpose<u32, 32>(a);
+      transpose<u32, 32>(b);
+#pragma unroll
+      for (int i = 0; i < 32; i++) {
+        u[64 * c + i] = a[i];
+        u[64 * c + 32 + i] = b[i];
+      }
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < W; c++) {
+      u64 a[64];
+#pragma unroll
+      for (int k = 0; k < 64; k++) a[k] = (k >= lo && k <= hi) ? ps.at(k, c, W) : 0ull;
+      transpose<u64, 64>(a);
+#pragma unroll
+      for (int i = 0; i < 64; i++)
+        if (64 * c + i < N) u[64 * c + i] = a[i];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Bit I/O.  Streams are 64-bit words, bits least-significant first
+// (zfp-rs src/bitstream/core.rs).
+// ---------------------------------------------------------------------------
+
+ZFPB_DEV u64 low_mask(u32 n) { return n < 64 ? (1ull << n) - 1 : ~0ull; }
+
+// Writes a block's bits from bit `pos` of `dst`.  With EDGE_ATOMIC the first
+// and the last (partial) word are OR-ed in atomically, for words shared with
+// the neighbouring blocks in a zeroed buffer; interior words are stored.
+// Words at or past `limit` are dropped (a block longer than its slot).
+template <bool EDGE_ATOMIC> struct Writer {
+  u64* dst;
+  u64 word;  // index of the word being filled
+  u64 limit;
+  u64 buf;
+  u32 bits;
+  bool first;
+
+  ZFPB_DEV void init(u64* d, u64 pos, u64 lim) {
+    dst = d;
+    word = pos >> 6;
+    limit = lim;
+    bits = (u32)(pos & 63);
+    buf = 0;
+    first = true;
+  }
+  ZFPB_DEV void emit(u64 w) {
+    if (word < limit) {
+      if (EDGE_ATOMIC && first)
+        atomicOr(dst + word, w);
+      else
+        dst[word] = w;
+    }
+    word++;
+    first = false;
+  }
+  // Append n <= 64 bits of v (no bits set above them).
+  ZFPB_DEV void put(u64 v, u32 n) {
+    buf |= v << bits;  // bits < 64
+    u32 total = bits + n;
+    if (total >= 64) {
+      emit(buf);
+      buf = (v >> 1) >> (63 - bits);
+      bits = total - 64;
+    } else {
+      bits = total;
+    }
+  }
+  ZFPB_DEV void put_zeros(u64 n) {
+    u64 total = bits + n;
+    while (total >= 64) {
+      emit(buf);
+      buf = 0;
+      total -= 64;
+    }
+    bits = (u32)total;
+  }
+  // Write out the partial last word.
+  ZFPB_DEV void finish() {
+    if (bits > 0 && word < limit) {
+      if (EDGE_ATOMIC)
+        atomicOr(dst + word, buf);
+      else
+        dst[word] = buf;
+    }
+  }
+  ZFPB_DEV u64 pos() const { return (word << 6) + bits; }
+};
+
+// Reads from bit `pos` of a stream of `len` words; words past the end read as
+// zero (core.rs:151-157).  Holds the current partial word and the next word.
+struct Reader {
+  const u64* src;
+  u64 len;
+  u64 word;  // index of the word after `nxt`
+  u64 buf;   // unread bits of the current word, `bits` of them
+  u64 nxt;   // the following word
+  u32 bits;
+
+  ZFPB_DEV u64 load(u64 i) const { return i < len ? __ldg(src + i) : 0ull; }
+  ZFPB_DEV void init(const u64* s, u64 n, u64 pos) {
+    src = s;
+    len = n;
+    u64 w = pos >> 6;
+    u32 off = (u32)(pos & 63);
+    if (off) {
+      buf = load(w) >> off;
+      bits = 64 - off;
+      nxt = load(w + 1);
+      word = w + 2;
+    } else {
+      buf = 0;
+      bits = 0;
+      nxt = load(w);
+      word = w + 1;
+    }
+  }
+  ZFPB_DEV u64 peek() const { return buf | (bits < 64 ? nxt << bits : 0ull); }
+  ZFPB_DEV void consume(u32 n) {
+    if (n <= bits) {
+      buf = n < 64 ? buf >> n : 0ull;
+      bits -= n;
+    } else {
+      u64 w = nxt;
+      nxt = load(word++);
+      bits = bits + 64 - n;
+      buf = (w >> 1) >> (63 - bits);
+    }
+  }
+  ZFPB_DEV u64 read(u32 n) {
+    u64 v = peek();
+    consume(n);
+    return v & low_mask(n);
+  }
+  ZFPB_DEV u32 read_bit() {
+    u32 b = (u32)(peek() & 1);
+    consume(1);
+    return b;
+  }
+  // Bit position of the cursor.
+  ZFPB_DEV u64 pos() const { return ((word - 1) << 6) - bits; }
+  // Skip n bits (n may exceed 64).
+  ZFPB_DEV void skip(u64 n) {
+    u64 p = pos() + n;
+    init(src, len, p);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Embedded bit-plane coder (bitplane.rs:509-790)
+// ---------------------------------------------------------------------------
+
+// Plane value of N <= 64 coefficients in one word; N = 256 in four.
+template <int N> struct PlaneOps {
+  static constexpr int W = N <= 64 ? 1 : N / 64;
+};
+
+// Lowest one-bit at or above n of plane words x[0..W): returns false if none.
+template <int W> ZFPB_DEV bool next_one(const u64* x, u32 n, u32* p) {
+  if constexpr (W == 1) {
+    u64 rest = n < 64 ? x[0] >> n : 0ull;
+    if (rest) { *p = n + (u32)__ffsll((long long)rest) - 1; return true; }
+    return false;
+  } else {
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+      if ((u32)(64 * j + 64) <= n) continue;
+      u64 v = x[j];
+      if ((u32)(64 * j) < n) v >>= (n - 64 * j), v <<= (n - 64 * j);
+      if (v) { *p = 64 * j + (u32)__ffsll((long long)v) - 1; return true; }
+    }
+    return false;
+  }
+}
+
+template <int W, class Wr> ZFPB_DEV void write_low(Wr& w, const u64* x, u32 m) {
+  if constexpr (W == 1) {
+    w.put(x[0] & low_mask(m), m);
+  } else {
+    u32 full = m >> 6, rest = m & 63;
+    for (u32 i = 0; i < full; i++) w.put(x[i], 64);
+    if (rest) w.put(x[full] & low_mask(rest), rest);
+  }
+}
+
+// encode_ints + encode_planes: code coefficients u (negabinary, in coding
+// order) under the budget; returns the bits written.
+template <class U, int N, class Wr>
+ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore ps) {
+  constexpr u32 intprec = sizeof(U) * 8;
+  constexpr u32 size = N;
+  constexpr int W = PlaneOps<N>::W;
+  const u32 budget = with_maxbits(maxbits, maxprec, size) ? maxbits : 0xffffffffu;
+  const u32 kmin = intprec > maxprec ? intprec - maxprec : 0;
+  U all = 0;
+#pragma unroll
+  for (int i = 0; i < N; i++) all |= u[i];
+  u32 top;
+  if constexpr (sizeof(U) == 4) top = 32 - __clz((int)all);
+  else top = 64 - __clzll((long long)all);
+  store_planes<U, N>(u, ps);
+
+  u32 bits = budget;
+  u32 n = 0;
+  u32 tk = top > kmin ? top : kmin;
+  u32 empty = intprec - tk;
+  empty = empty < bits ? empty : bits;
+  w.put_zeros(empty);
+  bits -= empty;
+  u32 k = intprec - empty;
+  while (bits != 0 && k > kmin) {
+    if (n == size) {
+      while (bits > size && k > kmin) {
+        k--;
+        u64 x[W];
+#pragma unroll
+        for (int c = 0; c < W; c++) x[c] = ps.at(k, c, W);
+        write_low<W>(w, x, size);
+        bits -= size;
+      }
+      if (k == kmin) break;
+    }
+    k--;
+    u64 x[W];
+#pragma unroll
+    for (int c = 0; c < W; c++) x[c] = ps.at(k, c, W);
+    u32 m = n < bits ? n : bits;
+    bits -= m;
+    write_low<W>(w, x, m);
+    while (bits != 0 && n < size) {
+      u32 p;
+      if (!next_one<W>(x, n, &p)) {
+        w.put(0, 1);
+        bits -= 1;
+        break;
+      }
+      u32 zeros = p - n;
+      bool last = p == size - 1;
+      u32 len = zeros + 2 - (last ? 1 : 0);
+      u32 take = len < bits ? len : bits;
+      if (take <= 64) {
+        u64 code = (last || zeros >= 63) ? 1ull : (1ull | (2ull << zeros));
+        w.put(code & low_mask(take), take);
+      } else {
+        w.put(1, 1);
+        w.put_zeros(zeros < take - 1 ? zeros : take - 1);
+        if (take == len && !last) w.put(1, 1);
+      }
+      bits -= take;
+      n = p + 1;
+    }
+  }
+  return budget - bits;
+}
+
+ZFPB_DEV u32 ctz64(u64 x) { return x ? (u32)__ffsll((long long)x) - 1 : 64u; }
+
+struct PlaneResult {
+  u32 bits, m, prec;
+  int low, high;  // stored planes are [low, high]; low = intprec if none
+};
+
+// decode_planes (bitplane.rs:675-790): planes go to the plane store.
+template <int N>
+ZFPB_DEV PlaneResult decode_planes(Reader& r, u32 budget, u32 kmin, u32 intprec, PlaneStore ps) {
+  constexpr u32 size = N;
+  constexpr int W = PlaneOps<N>::W;
+  u32 bits = budget, n = 0, m = 0, k = intprec;
+  int low = (int)intprec, high = -1;
+  while (bits != 0) {
+    m = 0;
+    if (k <= kmin) { k = k - 1; break; }
+    if (n == 0) {
+      u32 empty = ctz64(r.peek());
+      empty = empty < k - kmin ? empty : k - kmin;
+      empty = empty < bits ? empty : bits;
+      if (empty != 0) {
+        r.consume(empty);
+        bits -= empty;
+        k -= empty;
+        m = size;
+        continue;
+      }
+    } else if (n == size) {
+      while (bits > size && k > kmin) {
+        k--;
+#pragma unroll
+        for (int c = 0; c < W; c++) ps.at(k, c, W) = r.read(64 > size ? size : 64);
+        if (high < 0) high = (int)k;
+        bits -= size;
+        low = (int)k;
+      }
+      if (k == kmin) { k = k - 1; break; }
+    }
+    k--;
+    m = n < bits ? n : bits;
+    bits -= m;
+    u64 x[W];
+    if constexpr (W == 1) {
+      x[0] = r.read(m);
+    } else {
+#pragma unroll
+      for (int c = 0; c < W; c++) x[c] = 0;
+      u32 full = m >> 6, rest = m & 63;
+      for (u32 i = 0; i < full; i++) x[i] = r.read(64);
+      if (rest) x[full] = r.read(rest);
+    }
+    while (bits != 0 && n < size) {
+      u64 ahead = r.peek();
+      bits -= 1;
+      if ((ahead & 1) == 0) {
+        r.consume(1);
+        m = size;
+        break;
+      }
+      u32 limit = size - 1 - n;
+      limit = limit < bits ? limit : bits;
+      u32 zeros = ctz64(ahead >> 1);
+      u32 lim63 = limit < 63 ? limit : 63;
+      if (zeros < lim63) {
+        r.consume(zeros + 2);
+        bits -= zeros + 1;
+        n += zeros;
+      } else if (limit <= 63) {
+        r.consume(limit + 1);
+        bits -= limit;
+        n += limit;
+      } else {
+        r.consume(64);
+        bits -= 63;
+        n += 63;
+        u32 lim = limit - 63;
+        while (lim != 0) {  // scan_zeros, bitplane.rs:775-790
+          u32 z = ctz64(r.peek());
+          u32 span = lim < 64 ? lim : 64;
+          if (z < span) {
+            r.consume(z + 1);
+            bits -= z + 1;
+            n += z;
+            break;
+          }
+          r.consume(span);
+          bits -= span;
+          n += span;
+          lim -= span;
+        }
+      }
+      if constexpr (W == 1) x[0] |= 1ull << n;
+      else x[n >> 6] |= 1ull << (n & 63);
+      n += 1;
+      m = n;
+    }
+#pragma unroll
+    for (int c = 0; c < W; c++) ps.at(k, c, W) = x[c];
+    if (high < 0) high = (int)k;
+    low = (int)k;
+  }
+  if (n == 0) low = (int)intprec;
+  PlaneResult res;
+  res.bits = budget - bits;
+  res.m = m;
+  res.prec = intprec - k;
+  res.low = low;
+  res.high = high;
+  return res;
+}
+
+// decode_ints (bitplane.rs:626-667) into u; returns bits read, sets *zero.
+template <class U, int N>
+ZFPB_DEV u32 decode_ints(Reader& r, u32 maxbits, u32 maxprec, int rounding, U* u, bool* zero,
+                         PlaneStore ps) {
+  constexpr u32 intprec = sizeof(U) * 8;
+  const bool constrained = with_maxbits(maxbits, maxprec, N);
+  const u32 budget = constrained ? maxbits : 0xffffffffu;
+  const u32 kmin = intprec > maxprec ? intprec - maxprec : 0;
+  PlaneResult pr = decode_planes<N>(r, budget, kmin, intprec, ps);
+  bool z = pr.low == (int)intprec;
+  if (z) {
+#pragma unroll
+    for (int i = 0; i < N; i++) u[i] = 0;
+  } else {
+    load_planes<U, N>(u, ps, pr.low, pr.high);
+  }
+  bool round = rounding == 2;
+  if (round) {
+    u32 m = pr.m, prec = pr.prec;
+    if (!constrained) {
+      m = 0;
+      prec = intprec - (kmin - 1);
+    }
+    inv_round<U, N>(u, m, prec);
+  }
+  *zero = z && !round;
+  return pr.bits;
+}
+
+// ---------------------------------------------------------------------------
+// Block coders
+// ---------------------------------------------------------------------------
+
+template <int N> struct Dims { static constexpr u32 value = N == 4 ? 1 : N == 16 ? 2 : N == 64 ? 3 : 4; };
+
+// encode/integer.rs:50-93: transform, optional bias, reorder, planes, pad.
+template <class I, int N, class Wr>
+ZFPB_DEV u32 encode_int_block(Wr& w, I* b, u32 minbits, u32 maxbits, u32 maxprec, int rounding,
+                              PlaneStore ps) {
+  typedef typename Traits<I>::U U;
+  fwd_axes<I, N, 0>(b);
+  if (rounding == 1) fwd_round<I, N>(b, maxprec);
+  U u[N];
+  fwd_order<N>(u, b);
+  u32 bits = encode_ints<U, N>(w, maxbits, maxprec, u, ps);
+  if (bits < minbits) {
+    w.put_zeros(minbits - bits);
+    bits = minbits;
+  }
+  return bits;
+}
+
+// encode/float.rs:22-113
+template <class T, int N, class Wr>
+ZFPB_DEV u32 encode_float_block(Wr& w, const T* fb, const Codec& c, PlaneStore ps) {
+  typedef typename Traits<T>::I I;
+  int emax = exponent_block<T, N>(fb);
+  u32 prec = precision_f(emax, c.maxprec, c.minexp, Dims<N>::value, c.tight != 0);
+  u32 e = prec != 0 ? (u32)(emax + Traits<T>::EBIAS) : 0u;
+  if (e != 0) {
+    constexpr u32 hb = Traits<T>::EBITS + 1;
+    w.put(2 * (u64)e + 1, hb);
+    I ib[N];
+    fwd_cast<T, N>(ib, fb, emax);
+    return hb + encode_int_block<I, N>(w, ib, sat_sub(c.minbits, hb), sat_sub(c.maxbits, hb), prec,
+                                       c.rounding, ps);
+  }
+  w.put(0, 1);
+  if (c.minbits > 1) {
+    w.put_zeros(c.minbits - 1);
+    return c.minbits;
+  }
+  return 1;
+}
+
+// encode/reversible.rs:89-137
+template <class I, int N, class Wr>
+ZFPB_DEV u32 rev_encode_int_block(Wr& w, const I* ib, u32 maxbits, u32 maxprec, PlaneStore ps) {
+  typedef typename Traits<I>::U U;
+  constexpr u32 PB = sizeof(U) == 4 ? 5 : 6;
+  U u[N];
+  fwd_order<N>(u, ib);
+  U all = 0;
+#pragma unroll
+  for (int i = 0; i < N; i++) all |= u[i];
+  u32 prec;
+  if constexpr (sizeof(U) == 4) prec = all ? 32 - (u32)(__ffs((int)all) - 1) : 0;
+  else prec = all ? 64 - (u32)(__ffsll((long long)all) - 1) : 0;
+  prec = prec < maxprec ? prec : maxprec;
+  prec = prec < 1 ? 1 : prec;
+  w.put(prec - 1, PB);
+  return PB + encode_ints<U, N>(w, sat_sub(maxbits, PB), prec, u, ps);
+}
+
+// encode/reversible.rs:172-313
+template <class T, int N, class Wr>
+ZFPB_DEV u32 rev_encode_block(Wr& w, T* fb, const Codec& c, PlaneStore ps) {
+  typedef typename Traits<T>::I I;
+  typedef typename Traits<T>::U U;
+  u32 bits;
+  if constexpr (!Traits<T>::FLOAT) {
+    I* b = reinterpret_cast<I*>(fb);
+    fwd_axes<I, N, 2>(b);
+    bits = rev_encode_int_block<I, N>(w, b, c.maxbits, c.maxprec, ps);
+  } else {
+    int emax = exponent_block<T, N>(fb);
+    u32 e = (u32)(emax + Traits<T>::EBIAS);
+    bool tiny = e != 0 && emax < Traits<T>::MIN_CAST_EMAX;
+    I ib[N];
+#pragma unroll
+    for (int i = 0; i < N; i++) ib[i] = 0;
+    if (e != 0 && !tiny) fwd_cast<T, N>(ib, fb, emax);
+    bool rev = !tiny;
+    if (rev) {
+      constexpr int ip = Traits<T>::PREC;
+      T sc = pow2<T>(emax - (ip - 2));
+#pragma unroll
+      for (int i = 0; i < N; i++) rev = rev && (bits_of(mul_rn(sc, to_float(ib[i]))) == bits_of(fb[i]));
+    }
+    if (rev) {
+      if (e != 0) {
+        constexpr u32 hb = 2 + Traits<T>::EBITS;
+        w.put(1, 2);
+        w.put(e, Traits<T>::EBITS);
+        fwd_axes<I, N, 2>(ib);
+        bits = hb + rev_encode_int_block<I, N>(w, ib, sat_sub(c.maxbits, hb), c.maxprec, ps);
+      } else {
+        w.put(0, 1);
+        bits = 1;
+      }
+    } else {
+      const U tc = (U)(~(U)0) >> 1;
+#pragma unroll
+      for (int i = 0; i < N; i++) {
+        U b = (U)bits_of(fb[i]);
+        ib[i] = (b >> (sizeof(U) * 8 - 1)) ? (I)(b ^ tc) : (I)b;
+      }
+      w.put(3, 2);
+      fwd_axes<I, N, 2>(ib);
+      bits = 2 + rev_encode_int_block<I, N>(w, ib, sat_sub(c.maxbits, 2), c.maxprec, ps);
+    }
+  }
+  if (bits < c.minbits) {
+    w.put_zeros(c.minbits - bits);
+    bits = c.minbits;
+  }
+  return bits;
+}
+
+// Code one gathered block (codec/block/strided.rs dispatch).
+template <class T, int N, class Wr>
+ZFPB_DEV u32 encode_block(Wr& w, T* blk, const Codec& c, PlaneStore ps) {
+  if (c.minexp < ZFP_MIN_EXP) return rev_encode_block<T, N>(w, blk, c, ps);
+  if constexpr (Traits<T>::FLOAT) {
+    return encode_float_block<T, N>(w, blk, c, ps);
+  } else {
+    return encode_int_block<T, N>(w, blk, c.minbits, c.maxbits, c.maxprec, c.rounding, ps);
+  }
+}
+
+// ---- decoding -------------------------------------------------------------
+
+// decode/core.rs:97-131 (without the skip to minbits, which the caller does)
+template <class I, int N>
+ZFPB_DEV u32 decode_int_block(Reader& r, u32 maxbits, u32 maxprec, int rounding, I* ib, PlaneStore ps) {
+  typedef typename Traits<I>::U U;
+  U u[N];
+  bool zero;
+  u32 bits = decode_ints<U, N>(r, maxbits, maxprec, rounding, u, &zero, ps);
+  if (zero) {
+#pragma unroll
+    for (int i = 0; i < N; i++) ib[i] = 0;
+  } else {
+    inv_order<N>(u, ib);
+    inv_axes<I, N, 1>(ib);
+  }
+  return bits;
+}
+
+// decode/reversible.rs:46-82
+template <class I, int N>
+ZFPB_DEV u32 rev_decode_int_block(Reader& r, u32 maxbits, I* ib, PlaneStore ps) {
+  typedef typename Traits<I>::U U;
+  constexpr u32 PB = sizeof(U) == 4 ? 5 : 6;
+  u32 prec = (u32)r.read(PB) + 1;
+  U u[N];
+  bool zero;
+  u32 ub = decode_ints<U, N>(r, sat_sub(maxbits, PB), prec, 0, u, &zero, ps);
+  inv_order<N>(u, ib);
+  inv_axes<I, N, 3>(ib);
+  return PB + ub;
+}
+
+// Decode one block into blk; returns the bits the block occupies (after the
+// skip to minbits) and, in *read_bits, the bits actually read.
+template <class T, int N>
+ZFPB_DEV u32 decode_block(Reader& r, T* blk, const Codec& c, PlaneStore ps, u32* read_bits) {
+  typedef typename Traits<T>::I I;
+  typedef typename Traits<T>::U U;
+  u32 bits;
+  if (c.minexp < ZFP_MIN_EXP) {
+    if constexpr (!Traits<T>::FLOAT) {
+      bits = rev_decode_int_block<I, N>(r, c.maxbits, reinterpret_cast<I*>(blk), ps);
+    } else {
+      // decode/reversible.rs:130-194
+      if (r.read_bit() == 0) {
+#pragma unroll
+        for (int i = 0; i < N; i++) blk[i] = 0;
+        bits = 1;
+      } else {
+        bits = 2;
+        u32 reinterp = r.read_bit();
+        I ib[N];
+        if (reinterp) {
+          bits += rev_decode_int_block<I, N>(r, sat_sub(c.maxbits, bits), ib, ps);
+          const U tc = (U)(~(U)0) >> 1;
+#pragma unroll
+          for (int i = 0; i < N; i++) blk[i] = float_of(ib[i] < 0 ? (U)((U)ib[i] ^ tc) : (U)ib[i]);
+        } else {
+          int emax = (int)r.read(Traits<T>::EBITS) - Traits<T>::EBIAS;
+          bits += Traits<T>::EBITS;
+          bits += rev_decode_int_block<I, N>(r, sat_sub(c.maxbits, bits), ib, ps);
+          inv_cast<T, N>(ib, blk, emax);
+        }
+      }
+    }
+    *read_bits = bits;
+    return bits < c.minbits ? c.minbits : bits;
+  }
+  if constexpr (Traits<T>::FLOAT) {
+    // decode/core.rs:184-237
+    if (r.read_bit()) {
+      constexpr u32 hb = 1 + Traits<T>::EBITS;
+      int emax = (int)r.read(Traits<T>::EBITS) - Traits<T>::EBIAS;
+      u32 prec = precision_f(emax, c.maxprec, c.minexp, Dims<N>::value, c.tight != 0);
+      I ib[N];
+      u32 ibits = decode_int_block<I, N>(r, sat_sub(c.maxbits, hb), prec, c.rounding, ib, ps);
+      inv_cast<T, N>(ib, blk, emax);
+      u32 mb = sat_sub(c.minbits, hb);
+      *read_bits = hb + ibits;
+      return hb + (ibits < mb ? mb : ibits);
+    }
+#pragma unroll
+    for (int i = 0; i < N; i++) blk[i] = 0;
+    *read_bits = 1;
+    return c.minbits > 1 ? c.minbits : 1;
+  } else {
+    bits = decode_int_block<I, N>(r, c.maxbits, c.maxprec, c.rounding, blk, ps);
+    *read_bits = bits;
+    return bits < c.minbits ? c.minbits : bits;
+  }
+}
+
+}  // namespace zfpb

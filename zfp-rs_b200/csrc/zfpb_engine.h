@@ -1,0 +1,124 @@
+// Host-side engine interface between the C ABI (zfp_abi.cpp) and the CUDA
+// kernels.  Plain structs only; every pointer named d_* is device memory.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace zfpb {
+
+typedef unsigned long long u64;
+typedef unsigned int u32;
+typedef long long i64;
+
+// Field tiling in elements: data points at element [0,0,0,0] (field.rs:541-588).
+struct FieldGeom {
+  i64 s[4];    // effective strides
+  u64 n[4];    // dimensions
+  u64 b[4];    // blocks per axis
+  u64 nblocks;
+  int vec_ok;  // full-block rows are 16-byte aligned contiguous runs
+};
+
+enum : unsigned { FLAG_TRUNCATED = 1u, FLAG_BAD_INDEX = 2u };
+
+struct CodecParams {
+  u32 minbits, maxbits, maxprec;
+  int minexp;
+  int rounding;
+  int tight;
+};
+
+struct EncodeFixedArgs {
+  const void* data;
+  FieldGeom f;
+  CodecParams c;
+  u64* out;
+  u64 start;      // stream bit where the first block begins
+  u64 init_word;  // stream bits already in the start word, below start % 64
+  u64 blocks_per_cta;
+};
+
+struct EncodeVarArgs {
+  const void* data;
+  FieldGeom f;
+  CodecParams c;
+  u64* slots;
+  u64 slot_words;
+  u32* lengths;
+};
+
+struct DecodeArgs {
+  void* data;
+  FieldGeom f;
+  CodecParams c;
+  const u64* stream;
+  u64 stream_len;  // words
+  u64 start;
+  u64* offsets;    // nblocks + 1 entries, relative to start (variable path)
+  unsigned* flags;
+  // Fields whose strides may alias: owner[e - imin] is 1 + the last block (in
+  // stream order) that holds element e, and only that block stores it, so the
+  // result is that of a serial decode (zfp-rs decompress.rs:153-186).
+  u64* owner;
+  i64 imin;
+};
+
+// Whether two index tuples of the field can address the same element
+// (zfp-rs field_plan.rs:92-118).
+bool strides_may_alias(const FieldGeom& f, int dims);
+
+// One compress or decompress call.
+struct Call {
+  int type;  // 1 int32, 2 int64, 3 float, 4 double
+  int dims;  // 1..4
+  FieldGeom f;
+  CodecParams c;
+};
+
+// Result codes of the engine entry points.
+enum Status : int { OK = 0, ERR_OVERFLOW = 1, ERR_TRUNCATED = 2, ERR_CUDA = 3, ERR_ARGS = 4,
+                   // Candidate block offsets did not match the stream; call again without them.
+                   ERR_BAD_INDEX = 5 };
+
+// Whether every block takes exactly c.maxbits bits (minbits == maxbits and no
+// block can exceed the budget, zfp-rs config.rs:670-686).
+bool fixed_size_blocks(const Call& call);
+u32 block_bits(const CodecParams& c, int type, int dims);
+
+// Compress a device-resident field into d_out (cap words), from bit `start`
+// whose word already holds `init_word` below start % 64.  On OK, *end_bit is
+// the bit after the last block.  d_offsets (optional, nblocks + 1 entries)
+// receives each block's start relative to `start`.
+Status compress(const Call& call, const void* d_field, u64* d_out, u64 cap, u64 start, u64 init_word,
+                u64* end_bit, u64* d_offsets, cudaStream_t s);
+
+// Decompress into a device-resident field from d_in (len words) at bit
+// `start`.  d_offsets (optional) holds candidate block offsets; they are used
+// only if they check out as exactly those of a serial decode, else the call
+// returns ERR_BAD_INDEX (the field may be partly written).  Without them,
+// variable-size streams are walked for their offsets.  On OK or
+// ERR_TRUNCATED, *end_bit is the bit after the last block.
+Status decompress(const Call& call, const u64* d_in, u64 len, u64 start, void* d_field, u64* end_bit,
+                  const u64* d_offsets, cudaStream_t s);
+
+// Kernel launchers, one instantiation per scalar type (zfpb_inst_*.cu).
+template <class T> struct Launch {
+  static cudaError_t encode_fixed(const Call& call, const EncodeFixedArgs& a, u64 ctas, int threads,
+                                  size_t smem, cudaStream_t s);
+  static cudaError_t encode_var(const Call& call, const EncodeVarArgs& a, cudaStream_t s);
+  static cudaError_t decode_fixed(const Call& call, const DecodeArgs& a, cudaStream_t s);
+  static cudaError_t decode_var(const Call& call, const DecodeArgs& a, cudaStream_t s);
+  static cudaError_t walk(const Call& call, const DecodeArgs& a, cudaStream_t s);
+};
+
+// Per-kernel timing: events on the launching stream around every launch.
+void timing_enable(bool on);
+int timing_read(double* ms, unsigned long long* counts, int n);
+
+// Shared-memory bytes of plane storage per thread for a scalar type/dims.
+size_t plane_bytes(int type, int dims);
+
+}  // namespace zfpb

@@ -1,0 +1,91 @@
+// Kernel launchers for one scalar type; included once per type by
+// zfpb_inst_{i32,i64,f32,f64}.cu so the heavy templates compile in parallel.
+#pragma once
+
+#include "zfpb_kernels.cuh"
+
+namespace zfpb {
+
+template <class T, int D> static size_t plane_smem(int threads) {
+  return (size_t)KernelShape<T, D>::PLANE_WORDS * threads * sizeof(u64);
+}
+
+template <class T, int D> static cudaError_t set_smem(const void* fn, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+static inline unsigned grid_of(u64 n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+template <class T, int D>
+static cudaError_t encode_fixed_d(const EncodeFixedArgs& a, u64 ctas, int threads, size_t smem, cudaStream_t s) {
+  cudaError_t e = set_smem<T, D>((const void*)k_encode_fixed<T, D>, smem);
+  if (e != cudaSuccess) return e;
+  k_encode_fixed<T, D><<<(unsigned)ctas, threads, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <class T, int D> static int var_threads() { return D == 4 ? 32 : 128; }
+
+template <class T, int D> static cudaError_t encode_var_d(const EncodeVarArgs& a, cudaStream_t s) {
+  const int th = var_threads<T, D>();
+  size_t smem = plane_smem<T, D>(th);
+  cudaError_t e = set_smem<T, D>((const void*)k_encode_var<T, D>, smem);
+  if (e != cudaSuccess) return e;
+  k_encode_var<T, D><<<grid_of(a.f.nblocks, th), th, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <class T, int D> static cudaError_t decode_fixed_d(const DecodeArgs& a, cudaStream_t s) {
+  const int th = var_threads<T, D>();
+  size_t smem = plane_smem<T, D>(th);
+  cudaError_t e = set_smem<T, D>((const void*)k_decode_fixed<T, D>, smem);
+  if (e != cudaSuccess) return e;
+  k_decode_fixed<T, D><<<grid_of(a.f.nblocks, th), th, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <class T, int D> static cudaError_t decode_var_d(const DecodeArgs& a, cudaStream_t s) {
+  const int th = var_threads<T, D>();
+  size_t smem = plane_smem<T, D>(th);
+  cudaError_t e = set_smem<T, D>((const void*)k_decode_var<T, D>, smem);
+  if (e != cudaSuccess) return e;
+  k_decode_var<T, D><<<grid_of(a.f.nblocks, th), th, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <class T, int D> static cudaError_t walk_d(const DecodeArgs& a, cudaStream_t s) {
+  size_t smem = plane_smem<T, D>(1);
+  k_walk<T, D><<<1, 1, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+#define ZFPB_DISPATCH(call, fn, ...)             \
+  switch ((call).dims) {                         \
+    case 1: return fn<T, 1>(__VA_ARGS__);        \
+    case 2: return fn<T, 2>(__VA_ARGS__);        \
+    case 3: return fn<T, 3>(__VA_ARGS__);        \
+    default: return fn<T, 4>(__VA_ARGS__);       \
+  }
+
+template <class T>
+cudaError_t Launch<T>::encode_fixed(const Call& call, const EncodeFixedArgs& a, u64 ctas, int threads,
+                                    size_t smem, cudaStream_t s) {
+  ZFPB_DISPATCH(call, encode_fixed_d, a, ctas, threads, smem, s)
+}
+template <class T> cudaError_t Launch<T>::encode_var(const Call& call, const EncodeVarArgs& a, cudaStream_t s) {
+  ZFPB_DISPATCH(call, encode_var_d, a, s)
+}
+template <class T> cudaError_t Launch<T>::decode_fixed(const Call& call, const DecodeArgs& a, cudaStream_t s) {
+  ZFPB_DISPATCH(call, decode_fixed_d, a, s)
+}
+template <class T> cudaError_t Launch<T>::decode_var(const Call& call, const DecodeArgs& a, cudaStream_t s) {
+  ZFPB_DISPATCH(call, decode_var_d, a, s)
+}
+template <class T> cudaError_t Launch<T>::walk(const Call& call, const DecodeArgs& a, cudaStream_t s) {
+  ZFPB_DISPATCH(call, walk_d, a, s)
+}
+
+#undef ZFPB_DISPATCH
+
+}  // namespace zfpb

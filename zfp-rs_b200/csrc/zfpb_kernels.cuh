@@ -1,0 +1,397 @@
+// Field-level kernels: block tiling (zfp-rs src/field_plan.rs:41-206), the
+// gather/scatter of 4^d tiles (encode/dim{1..4}.rs, decode/dim{1..4}.rs), and
+// one thread per block driving the block codec of zfpb_block.cuh.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "zfpb_block.cuh"
+#include "zfpb_engine.h"
+
+namespace zfpb {
+
+// Block index -> origin element offset and per-axis lengths (1..4), for
+// blocks in row-major order with x fastest (field_plan.rs:128-200).
+template <int D>
+ZFPB_DEV i64 block_origin(const FieldGeom& f, u64 idx, int* len) {
+  i64 off = 0;
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    u64 nb = f.b[d];
+    u64 c = (d == D - 1) ? idx : idx % nb;
+    idx = (d == D - 1) ? 0 : idx / nb;
+    u64 o = 4 * c;
+    off += (i64)o * f.s[d];
+    u64 r = f.n[d] - o;
+    len[d] = r < 4 ? (int)r : 4;
+  }
+  return off;
+}
+
+// Load four values of a row at stride sx; vectorised when the row is a
+// 16-byte aligned contiguous run.
+template <class T> ZFPB_DEV void load_row(const T* p, i64 sx, bool vec, T* v) {
+  if (vec) {
+    if constexpr (sizeof(T) == 4) {
+      int4 q = __ldg(reinterpret_cast<const int4*>(p));
+      v[0] = *reinterpret_cast<const T*>(&q.x);
+      v[1] = *reinterpret_cast<const T*>(&q.y);
+      v[2] = *reinterpret_cast<const T*>(&q.z);
+      v[3] = *reinterpret_cast<const T*>(&q.w);
+    } else {
+      longlong2 a = __ldg(reinterpret_cast<const longlong2*>(p));
+      longlong2 b = __ldg(reinterpret_cast<const longlong2*>(p) + 1);
+      v[0] = *reinterpret_cast<const T*>(&a.x);
+      v[1] = *reinterpret_cast<const T*>(&a.y);
+      v[2] = *reinterpret_cast<const T*>(&b.x);
+      v[3] = *reinterpret_cast<const T*>(&b.y);
+    }
+  } else {
+#pragma unroll
+    for (int x = 0; x < 4; x++) v[x] = __ldg(p + x * sx);
+  }
+}
+
+template <class T> ZFPB_DEV void store_row(T* p, i64 sx, bool vec, const T* v) {
+  if (vec) {
+    if constexpr (sizeof(T) == 4) {
+      int4 q;
+      q.x = *reinterpret_cast<const int*>(&v[0]);
+      q.y = *reinterpret_cast<const int*>(&v[1]);
+      q.z = *reinterpret_cast<const int*>(&v[2]);
+      q.w = *reinterpret_cast<const int*>(&v[3]);
+      *reinterpret_cast<int4*>(p) = q;
+    } else {
+      longlong2 a, b;
+      a.x = *reinterpret_cast<const long long*>(&v[0]);
+      a.y = *reinterpret_cast<const long long*>(&v[1]);
+      b.x = *reinterpret_cast<const long long*>(&v[2]);
+      b.y = *reinterpret_cast<const long long*>(&v[3]);
+      reinterpret_cast<longlong2*>(p)[0] = a;
+      reinterpret_cast<longlong2*>(p)[1] = b;
+    }
+  } else {
+#pragma unroll
+    for (int x = 0; x < 4; x++) p[x * sx] = v[x];
+  }
+}
+
+// Gather a (possibly partial) block with C pad_block padding
+// (encode/dim3.rs:44-78, encode/core.rs:194-219): x within filled rows, then
+// y, then z, then w; a padded entry copies entry 0, 1, 0 of its run for
+// positions 1, 2, 3.
+template <class T, int D>
+ZFPB_DEV void gather_block(const T* base, const FieldGeom& f, i64 off, const int* len, T* b) {
+  constexpr int N = 1 << (2 * D);
+  const T* p = base + off;
+  bool full = true;
+#pragma unroll
+  for (int d = 0; d < D; d++) full = full && len[d] == 4;
+  if (full) {
+    const bool vec = f.vec_ok != 0;
+#pragma unroll
+    for (int r = 0; r < N / 4; r++) {
+      i64 o = 0;
+      if (D > 1) o += (i64)(r & 3) * f.s[1];
+      if (D > 2) o += (i64)((r >> 2) & 3) * f.s[2];
+      if (D > 3) o += (i64)(r >> 4) * f.s[3];
+      load_row<T>(p + o, f.s[0], vec, b + 4 * r);
+    }
+    return;
+  }
+  const int nx = len[0], ny = D > 1 ? len[1] : 1, nz = D > 2 ? len[2] : 1, nw = D > 3 ? len[3] : 1;
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    const int x = i & 3, y = (i >> 2) & 3, z = (i >> 4) & 3, w = i >> 6;
+    T v = 0;
+    if (x < nx && y < ny && z < nz && w < nw) {
+      i64 o = (i64)x * f.s[0];
+      if (D > 1) o += (i64)y * f.s[1];
+      if (D > 2) o += (i64)z * f.s[2];
+      if (D > 3) o += (i64)w * f.s[3];
+      v = __ldg(p + o);
+    }
+    b[i] = v;
+  }
+  // x within rows
+#pragma unroll
+  for (int r = 0; r < N / 4; r++) {
+    T* q = b + 4 * r;
+    if (nx <= 1) q[1] = q[0];
+    if (nx <= 2) q[2] = q[1];
+    if (nx <= 3) q[3] = q[0];
+  }
+  if constexpr (D >= 2) {
+#pragma unroll
+    for (int g = 0; g < N / 16; g++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        T* q = b + 16 * g + x;
+        if (ny <= 1) q[4] = q[0];
+        if (ny <= 2) q[8] = q[4];
+        if (ny <= 3) q[12] = q[0];
+      }
+  }
+  if constexpr (D >= 3) {
+#pragma unroll
+    for (int g = 0; g < N / 64; g++)
+#pragma unroll
+      for (int x = 0; x < 16; x++) {
+        T* q = b + 64 * g + x;
+        if (nz <= 1) q[16] = q[0];
+        if (nz <= 2) q[32] = q[16];
+        if (nz <= 3) q[48] = q[0];
+      }
+  }
+  if constexpr (D >= 4) {
+#pragma unroll
+    for (int x = 0; x < 64; x++) {
+      T* q = b + x;
+      if (nw <= 1) q[64] = q[0];
+      if (nw <= 2) q[128] = q[64];
+      if (nw <= 3) q[192] = q[0];
+    }
+  }
+}
+
+// Store the in-field part of a block (decode/dim3.rs:221-260).  With an
+// owner map, an element is stored only by the block that owns it.
+template <class T, int D>
+ZFPB_DEV void scatter_block(T* base, const FieldGeom& f, i64 off, const int* len, const T* b,
+                            const u64* owner = nullptr, i64 imin = 0, u64 blk = 0) {
+  constexpr int N = 1 << (2 * D);
+  T* p = base + off;
+  bool full = true;
+#pragma unroll
+  for (int d = 0; d < D; d++) full = full && len[d] == 4;
+  if (owner) {
+    const int nx = len[0], ny = D > 1 ? len[1] : 1, nz = D > 2 ? len[2] : 1, nw = D > 3 ? len[3] : 1;
+    for (int i = 0; i < N; i++) {
+      const int x = i & 3, y = (i >> 2) & 3, z = (i >> 4) & 3, w = i >> 6;
+      if (x < nx && y < ny && z < nz && w < nw) {
+        i64 o = (i64)x * f.s[0];
+        if (D > 1) o += (i64)y * f.s[1];
+        if (D > 2) o += (i64)z * f.s[2];
+        if (D > 3) o += (i64)w * f.s[3];
+        if (owner[off + o - imin] == blk + 1) p[o] = b[i];
+      }
+    }
+    return;
+  }
+  if (full) {
+    const bool vec = f.vec_ok != 0;
+#pragma unroll
+    for (int r = 0; r < N / 4; r++) {
+      i64 o = 0;
+      if (D > 1) o += (i64)(r & 3) * f.s[1];
+      if (D > 2) o += (i64)((r >> 2) & 3) * f.s[2];
+      if (D > 3) o += (i64)(r >> 4) * f.s[3];
+      store_row<T>(p + o, f.s[0], vec, b + 4 * r);
+    }
+    return;
+  }
+  const int nx = len[0], ny = D > 1 ? len[1] : 1, nz = D > 2 ? len[2] : 1, nw = D > 3 ? len[3] : 1;
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    const int x = i & 3, y = (i >> 2) & 3, z = (i >> 4) & 3, w = i >> 6;
+    if (x < nx && y < ny && z < nz && w < nw) {
+      i64 o = (i64)x * f.s[0];
+      if (D > 1) o += (i64)y * f.s[1];
+      if (D > 2) o += (i64)z * f.s[2];
+      if (D > 3) o += (i64)w * f.s[3];
+      p[o] = b[i];
+    }
+  }
+}
+
+template <class T, int D> struct KernelShape {
+  static constexpr int N = 1 << (2 * D);
+  static constexpr int W = N <= 64 ? 1 : N / 64;
+  static constexpr int PREC = Traits<T>::PREC;
+  // Shared-memory words of plane storage per thread.
+  static constexpr int PLANE_WORDS = PREC * W;
+};
+
+// ---------------------------------------------------------------------------
+// Fixed-size blocks (every block exactly maxbits bits): stage a CTA's bits in
+// shared memory, then store the stream words the CTA owns.  CTA j codes blocks
+// [jB, jB + B + X): the X extra blocks are the next CTA's first ones, which
+// complete the last word this CTA owns.  A CTA owns the words whose first bit
+// lies in its own bit range; CTA 0 also owns the word holding the start bit,
+// into which it merges the bits already in the stream.
+// ---------------------------------------------------------------------------
+template <class T, int D>
+__global__ void __launch_bounds__(128, 1) k_encode_fixed(EncodeFixedArgs a) {
+  typedef KernelShape<T, D> S;
+  extern __shared__ u64 smem[];
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  PlaneStore ps{smem + tid, nthr};
+  u64* stage = smem + (size_t)S::PLANE_WORDS * nthr;
+  const u64 maxbits = a.c.maxbits;
+  const u64 first = (u64)blockIdx.x * a.blocks_per_cta;
+  const u64 g0 = a.start + first * maxbits;
+  const u64 w0 = g0 >> 6;
+  const u32 lb = (u32)(g0 & 63);
+  const u32 stage_words = (u32)((lb + (u64)nthr * maxbits + 63) >> 6) + 1;
+  for (u32 i = tid; i < stage_words; i += nthr) stage[i] = 0;
+  __syncthreads();
+
+  const u64 blk = first + tid;
+  if (blk < a.f.nblocks) {
+    int len[4];
+    i64 off = block_origin<D>(a.f, blk, len);
+    T b[S::N];
+    gather_block<T, D>(static_cast<const T*>(a.data), a.f, off, len, b);
+    Writer<true> w;
+    w.init(stage, lb + (u64)tid * maxbits, stage_words);
+    encode_block<T, S::N>(w, b, a.c, ps);
+    w.finish();
+  }
+  __syncthreads();
+
+  const u64 nb = a.f.nblocks - first < a.blocks_per_cta ? a.f.nblocks - first : a.blocks_per_cta;
+  u64 lo = (g0 + 63) >> 6;
+  const u64 hi = (g0 + nb * maxbits + 63) >> 6;
+  if (blockIdx.x == 0 && lb != 0) lo = w0;
+  for (u64 wi = lo + tid; wi < hi; wi += nthr) {
+    u64 v = stage[wi - w0];
+    if (blockIdx.x == 0 && wi == w0) v |= a.init_word;
+    a.out[wi] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Variable-size blocks, pass 1: each block coded into its own slot of the
+// scratch buffer (slot i at word i * slot_words), its bit length recorded.
+// ---------------------------------------------------------------------------
+template <class T, int D>
+__global__ void __launch_bounds__(128, 1) k_encode_var(EncodeVarArgs a) {
+  typedef KernelShape<T, D> S;
+  extern __shared__ u64 smem[];
+  const int tid = threadIdx.x;
+  PlaneStore ps{smem + tid, (int)blockDim.x};
+  const u64 blk = (u64)blockIdx.x * blockDim.x + tid;
+  if (blk >= a.f.nblocks) return;
+  int len[4];
+  i64 off = block_origin<D>(a.f, blk, len);
+  T b[S::N];
+  gather_block<T, D>(static_cast<const T*>(a.data), a.f, off, len, b);
+  Writer<false> w;
+  w.init(a.slots + blk * a.slot_words, 0, a.slot_words);
+  u32 bits = encode_block<T, S::N>(w, b, a.c, ps);
+  w.finish();
+  a.lengths[blk] = bits;
+}
+
+// Truncation rule (zfp-rs decompress.rs:57-74, bitstream/core.rs:377-404): a
+// stream is truncated when decoding loaded a word past its end: a word holding
+// a bit that was read, or the word a skip to a block's padded end landed in
+// (when not at a word boundary).
+ZFPB_DEV void check_loads(u64 start, u32 read_bits, u32 occupied, u64 len, unsigned* flags) {
+  u64 last = 0;
+  bool any = false;
+  if (read_bits > 0) {
+    last = (start + read_bits - 1) >> 6;
+    any = true;
+  }
+  u64 end = start + occupied;
+  if (occupied > read_bits && (end & 63) != 0) {
+    u64 wv = end >> 6;
+    last = any && last > wv ? last : wv;
+    any = true;
+  }
+  if (any && last >= len) atomicOr(flags, FLAG_TRUNCATED);
+}
+
+// Fixed-size blocks: block i starts at start + i * maxbits (decompress.rs:205-330).
+template <class T, int D>
+__global__ void __launch_bounds__(128, 1) k_decode_fixed(DecodeArgs a) {
+  typedef KernelShape<T, D> S;
+  extern __shared__ u64 smem[];
+  const int tid = threadIdx.x;
+  PlaneStore ps{smem + tid, (int)blockDim.x};
+  const u64 blk = (u64)blockIdx.x * blockDim.x + tid;
+  if (blk >= a.f.nblocks) return;
+  const u64 pos = a.start + blk * (u64)a.c.maxbits;
+  Reader r;
+  r.init(a.stream, a.stream_len, pos);
+  T b[S::N];
+  u32 rb;
+  u32 occ = decode_block<T, S::N>(r, b, a.c, ps, &rb);
+  check_loads(pos, rb, occ, a.stream_len, a.flags);
+  int len[4];
+  i64 off = block_origin<D>(a.f, blk, len);
+  scatter_block<T, D>(static_cast<T*>(a.data), a.f, off, len, b, a.owner, a.imin, blk);
+}
+
+// Variable-size blocks with known offsets: decode each block from its offset
+// and check that it ends where the next begins, which makes the offsets
+// exactly those of a serial decode (else FLAG_BAD_INDEX).
+template <class T, int D>
+__global__ void __launch_bounds__(128, 1) k_decode_var(DecodeArgs a) {
+  typedef KernelShape<T, D> S;
+  extern __shared__ u64 smem[];
+  const int tid = threadIdx.x;
+  PlaneStore ps{smem + tid, (int)blockDim.x};
+  const u64 blk = (u64)blockIdx.x * blockDim.x + tid;
+  if (blk >= a.f.nblocks) return;
+  const u64 o0 = a.offsets[blk], o1 = a.offsets[blk + 1];
+  const u64 pos = a.start + o0;
+  Reader r;
+  r.init(a.stream, a.stream_len, pos);
+  T b[S::N];
+  u32 rb;
+  u32 occ = decode_block<T, S::N>(r, b, a.c, ps, &rb);
+  if (o1 < o0 || (u64)occ != o1 - o0) {
+    atomicOr(a.flags, FLAG_BAD_INDEX);
+    return;
+  }
+  check_loads(pos, rb, occ, a.stream_len, a.flags);
+  int len[4];
+  i64 off = block_origin<D>(a.f, blk, len);
+  scatter_block<T, D>(static_cast<T*>(a.data), a.f, off, len, b, a.owner, a.imin, blk);
+}
+
+// Offsets of a stream without an index: one thread decodes block after block,
+// as the serial reader does (decompress/pipeline.rs:139-171), recording where
+// each starts.  offsets[i] is relative to the start bit; offsets[n] is the end.
+template <class T, int D>
+__global__ void __launch_bounds__(32) k_walk(DecodeArgs a) {
+  typedef KernelShape<T, D> S;
+  extern __shared__ u64 smem[];
+  if (threadIdx.x != 0) return;
+  PlaneStore ps{smem, 1};
+  u64 rel = 0;
+  for (u64 blk = 0; blk < a.f.nblocks; blk++) {
+    a.offsets[blk] = rel;
+    Reader r;
+    r.init(a.stream, a.stream_len, a.start + rel);
+    T b[S::N];
+    u32 rb;
+    u32 occ = decode_block<T, S::N>(r, b, a.c, ps, &rb);
+    rel += occ;
+  }
+  a.offsets[a.f.nblocks] = rel;
+}
+
+// Owner map for fields whose strides may alias: every element records the
+// last block, in stream order, that holds it.
+template <int D> __global__ void k_claim(FieldGeom f, u64* owner, i64 imin) {
+  const u64 blk = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (blk >= f.nblocks) return;
+  int len[4];
+  i64 off = block_origin<D>(f, blk, len);
+  const int nx = len[0], ny = D > 1 ? len[1] : 1, nz = D > 2 ? len[2] : 1, nw = D > 3 ? len[3] : 1;
+  for (int w = 0; w < nw; w++)
+    for (int z = 0; z < nz; z++)
+      for (int y = 0; y < ny; y++)
+        for (int x = 0; x < nx; x++) {
+          i64 o = (i64)x * f.s[0];
+          if (D > 1) o += (i64)y * f.s[1];
+          if (D > 2) o += (i64)z * f.s[2];
+          if (D > 3) o += (i64)w * f.s[3];
+          atomicMax(owner + (off + o - imin), blk + 1);
+        }
+}
+
+}  // namespace zfpb
