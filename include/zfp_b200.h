@@ -22,7 +22,8 @@ zfp_bool zfp_stream_set_rounding(zfp_stream* stream, int rounding, zfp_bool tigh
 int zfp_stream_rounding(const zfp_stream* stream, zfp_bool* tight_error);
 
 /* Status of the last failed call on this thread: 0 none, 1 buffer too small,
- * 2 truncated stream, 3 CUDA error, 4 invalid arguments. */
+ * 2 truncated stream, 3 CUDA error, 4 invalid arguments, 6 field too large
+ * for zfpb_compress_device_noalloc. */
 int zfpb_last_error(void);
 
 /* A field and codec parameters in one plain struct for the device API. */
@@ -53,6 +54,28 @@ size_t zfpb_compress_device(const zfpb_desc* desc, const void* d_field, void* d_
  * Returns the bytes consumed, or 0 on failure (e.g. a truncated stream). */
 size_t zfpb_decompress_device(const zfpb_desc* desc, const void* d_stream, size_t bytes, void* d_field,
                               const uint64_t* d_block_offsets, void* cuda_stream);
+
+/* Compress without allocating device memory.
+ *
+ * No counterpart in the reference: zfp-rs allocates its chunk buffers itself.
+ * This entry point is for callers that cannot have the library call
+ * cudaMalloc: a host application that has reserved all of its device memory
+ * for its own pool (so an allocation would fail or evict its data), or a
+ * latency-critical loop that cannot absorb cudaMalloc's implicit device-wide
+ * synchronization.  It behaves as zfpb_compress_device (same stream bytes,
+ * no header, no index) but takes its scratch from a fixed 16 MiB device array
+ * inside the library, which every device that loads the library holds until
+ * the process exits.  Limit: fields whose variable-rate scratch (one slot of
+ * zfp_block_maximum_size bits per block, plus 12 bytes per block) exceeds
+ * 16 MiB are rejected: the call returns 0 and zfpb_last_error() returns 6.
+ * Fixed-size blocks (fixed-rate mode) need no scratch and have no limit.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the array: calls
+ * whose kernels overlap on the GPU (from several host threads or streams)
+ * race and must be serialized by the caller.  The call returns once the
+ * stream is complete. */
+size_t zfpb_compress_device_noalloc(const zfpb_desc* desc, const void* d_field, void* d_stream,
+                                    size_t capacity, void* cuda_stream);
 
 /* Per-kernel timing for profiling: when enabled, every kernel launch of the
  * library is bracketed by CUDA events on its stream.  zfpb_timing_enable

@@ -1285,3 +1285,19 @@ extern "C" size_t zfpb_decompress_device(const zfpb_desc* d, const void* d_strea
   if (cudaStreamSynchronize(s) != cudaSuccess) return fail(zfpb::ERR_CUDA);
   return (size_t)((end + 63) / 64 * 8);
 }
+
+// Same stream as zfpb_compress_device, with scratch from the library's static
+// device array instead of cudaMalloc (see include/zfp_b200.h).  Allocates
+// nothing: no cudaMalloc, cudaFree, cudaMallocHost or library allocator.
+extern "C" size_t zfpb_compress_device_noalloc(const zfpb_desc* d, const void* d_field, void* d_stream,
+                                               size_t capacity, void* cuda_stream) {
+  if (!d || !d_field || !d_stream || ((uintptr_t)d_stream % 8) != 0) return fail(zfpb::ERR_ARGS);
+  Plan p;
+  zfpb::Call call;
+  if (!call_of_desc(d, p, call, d_field)) return fail(zfpb::ERR_ARGS);
+  u64 end = 0;
+  zfpb::Status st = zfpb::compress_noalloc(call, d_field, (u64*)d_stream, capacity / 8, &end,
+                                           (cudaStream_t)cuda_stream);
+  if (st != zfpb::OK) return fail(st);
+  return (size_t)((end + 63) / 64 * 8);
+}

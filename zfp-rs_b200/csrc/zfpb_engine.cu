@@ -586,3 +586,124 @@ Status decompress(const Call& call, const u64* d_in, u64 len, u64 start, void* d
 }
 
 }  // namespace zfpb
+
+// ---------------------------------------------------------------------------
+// Compression without device allocation (zfpb_compress_device_noalloc).
+//
+// Its scratch (block slots, bit lengths, block offsets, scan totals) is this
+// file-scope device array instead of cudaMalloc'd workspace.  Every device
+// that loads the library holds the array until the process exits.  Calls
+// share it and leave their contents in it; nothing in it needs to start at
+// zero, because every word a call reads was written earlier in that same call.
+// Two calls whose kernels overlap on the GPU (different host threads or
+// streams) race on the array.
+// ---------------------------------------------------------------------------
+
+namespace zfpb {
+
+static constexpr u64 NOALLOC_SCRATCH_WORDS = 1ull << 21;  // 16 MiB
+static __device__ __align__(256) u64 g_noalloc_scratch[NOALLOC_SCRATCH_WORDS];
+
+static std::mutex g_noalloc_mu;
+static u64* g_noalloc_ptr[64];
+
+u64 noalloc_scratch_bytes() { return NOALLOC_SCRATCH_WORDS * sizeof(u64); }
+
+// The array's device address for the current device, looked up on the first
+// call on that device.  In host code the array's name is only a host-side
+// stand-in, never a device address.
+static Status noalloc_scratch(u64** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return ERR_CUDA;
+  std::lock_guard<std::mutex> l(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) {
+      cudaGetLastError();
+      return ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = static_cast<u64*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return OK;
+}
+
+Status compress_noalloc(const Call& call, const void* d_field, u64* d_out, u64 cap, u64* end_bit,
+                        cudaStream_t s) {
+  const u64 n = call.f.nblocks;
+  *end_bit = 0;
+  if (n == 0) return OK;
+  if (fixed_size_blocks(call)) {
+    // Fixed-size blocks need no scratch: the same kernel as compress().
+    const u64 maxbits = call.c.maxbits;
+    const u64 end = n * maxbits;
+    if ((end + 63) / 64 > cap) return ERR_OVERFLOW;
+    int threads;
+    u64 per_cta;
+    size_t smem;
+    if (fixed_shape(call, &threads, &per_cta, &smem)) {
+      EncodeFixedArgs a;
+      a.data = d_field;
+      a.f = call.f;
+      a.c = call.c;
+      a.out = d_out;
+      a.start = 0;
+      a.init_word = 0;
+      a.blocks_per_cta = per_cta;
+      u64 ctas = (n + per_cta - 1) / per_cta;
+      ZFPB_CHECK(for_type(call.type, [&](auto* tp) {
+        using T = std::remove_pointer_t<decltype(tp)>;
+        return Launch<T>::encode_fixed(call, a, ctas, threads, smem, s);
+      }));
+      ZFPB_CHECK(cudaStreamSynchronize(s));
+      *end_bit = end;
+      return OK;
+    }
+  }
+  u64* scratch = nullptr;
+  Status st = noalloc_scratch(&scratch);
+  if (st != OK) return st;
+  const u64 bb = block_bits(call.c, call.type, call.dims);
+  const u64 slot_words = (bb + 63) / 64 + 1;
+  const u64 tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  const u64 w_slots = n * slot_words + 1, w_len = (n + 1) / 2, w_off = n + 1, w_part = tiles + 1;
+  if (w_slots + w_len + w_off + w_part > NOALLOC_SCRATCH_WORDS) return ERR_TOO_LARGE;
+  u64* slots = scratch;
+  u32* lengths = reinterpret_cast<u32*>(scratch + w_slots);
+  u64* off = scratch + w_slots + w_len;
+  u64* part = off + w_off;
+  EncodeVarArgs ea;
+  ea.data = d_field;
+  ea.f = call.f;
+  ea.c = call.c;
+  ea.slots = slots;
+  ea.slot_words = slot_words;
+  ea.lengths = lengths;
+  ZFPB_CHECK(for_type(call.type, [&](auto* tp) {
+    using T = std::remove_pointer_t<decltype(tp)>;
+    return Launch<T>::encode_var(call, ea, s);
+  }));
+  k_scan_reduce<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(lengths, n, part);
+  k_scan_partials<<<1, 1024, 0, s>>>(part, tiles, off + n);
+  k_scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(lengths, n, part, off);
+  ZFPB_CHECK(cudaGetLastError());
+  u64 total = 0;
+  ZFPB_CHECK(cudaMemcpyAsync(&total, off + n, sizeof(u64), cudaMemcpyDeviceToHost, s));
+  ZFPB_CHECK(cudaStreamSynchronize(s));
+  *end_bit = total;
+  if ((total + 63) / 64 > cap) return ERR_OVERFLOW;
+  PackArgs pa;
+  pa.slots = slots;
+  pa.slot_words = slot_words;
+  pa.off = off;
+  pa.nblocks = n;
+  pa.start = 0;
+  pa.init_word = 0;
+  pa.out = d_out;
+  k_pack<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pa);
+  ZFPB_CHECK(cudaGetLastError());
+  ZFPB_CHECK(cudaStreamSynchronize(s));
+  return OK;
+}
+
+}  // namespace zfpb

@@ -81,7 +81,9 @@ struct Call {
 // Result codes of the engine entry points.
 enum Status : int { OK = 0, ERR_OVERFLOW = 1, ERR_TRUNCATED = 2, ERR_CUDA = 3, ERR_ARGS = 4,
                    // Candidate block offsets did not match the stream; call again without them.
-                   ERR_BAD_INDEX = 5 };
+                   ERR_BAD_INDEX = 5,
+                   // The field needs more scratch than the no-allocation entry point has.
+                   ERR_TOO_LARGE = 6 };
 
 // Whether every block takes exactly c.maxbits bits (minbits == maxbits and no
 // block can exceed the budget, zfp-rs config.rs:670-686).
@@ -113,6 +115,13 @@ template <class T> struct Launch {
   static cudaError_t decode_var(const Call& call, const DecodeArgs& a, cudaStream_t s);
   static cudaError_t walk(const Call& call, const DecodeArgs& a, cudaStream_t s);
 };
+
+// Compress from bit 0 of d_out (cap words) without allocating device memory:
+// scratch is a fixed static device array of noalloc_scratch_bytes() bytes.
+// Returns ERR_TOO_LARGE for a field whose scratch does not fit.  Synchronous.
+Status compress_noalloc(const Call& call, const void* d_field, u64* d_out, u64 cap, u64* end_bit,
+                        cudaStream_t s);
+u64 noalloc_scratch_bytes();
 
 // Per-kernel timing: events on the launching stream around every launch.
 void timing_enable(bool on);

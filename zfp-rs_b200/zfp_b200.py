@@ -28,7 +28,8 @@ HEADER_MAGIC, HEADER_META, HEADER_MODE, HEADER_FULL = 1, 2, 4, 7
 TYPE_CODE = {np.dtype(np.int32): 1, np.dtype(np.int64): 2, np.dtype(np.float32): 3, np.dtype(np.float64): 4}
 CODE_TYPE = {v: k for k, v in TYPE_CODE.items()}
 ROUND_NEVER, ROUND_FIRST, ROUND_LAST = 0, -1, 1
-ERRORS = {1: "buffer too small", 2: "stream is truncated", 3: "CUDA error", 4: "invalid arguments"}
+ERRORS = {1: "buffer too small", 2: "stream is truncated", 3: "CUDA error", 4: "invalid arguments",
+          6: "field too large for the no-allocation scratch"}
 
 
 class ZfpError(RuntimeError):
@@ -129,6 +130,7 @@ SIGNATURES = [
     ("zfpb_timing_read", C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_ulonglong), C.c_int]),
     ("zfpb_compress_device", _sz, [C.POINTER(ZfpDesc), _vp, _vp, _sz, _vp, _vp]),
     ("zfpb_decompress_device", _sz, [C.POINTER(ZfpDesc), _vp, _sz, _vp, _vp, _vp]),
+    ("zfpb_compress_device_noalloc", _sz, [C.POINTER(ZfpDesc), _vp, _vp, _sz, _vp]),
 ]
 DATA_SYMBOLS = ["stream_word_bits", "zfp_codec_version", "zfp_library_version"]
 
