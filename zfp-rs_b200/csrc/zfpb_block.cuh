@@ -650,10 +650,10 @@ template <int W, class Wr> ZFPB_DEV void write_low(Wr& w, const u64* x, u32 m) {
   }
 }
 
-// encode_ints + encode_planes: code coefficients u (negabinary, in coding
-// order) under the budget; returns the bits written.
+// encode_ints + encode_planes one group test at a time (bitplane.rs:509-610);
+// used for 4-D blocks, whose planes are 256 bits wide.
 template <class U, int N, class Wr>
-ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore ps) {
+ZFPB_DEV u32 encode_ints_loop(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore ps) {
   constexpr u32 intprec = sizeof(U) * 8;
   constexpr u32 size = N;
   constexpr int W = PlaneOps<N>::W;
@@ -718,6 +718,129 @@ ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore
     }
   }
   return budget - bits;
+}
+
+// kOnesDoubled[b]: the bits of byte b, least significant first, with every
+// one-bit written twice ("1" -> "11"); at most 16 bits.
+__device__ const unsigned short kOnesDoubled[256] = {
+    0x0000, 0x0003, 0x0006, 0x000f, 0x000c, 0x001b, 0x001e, 0x003f, 0x0018, 0x0033, 0x0036, 0x006f,
+    0x003c, 0x007b, 0x007e, 0x00ff, 0x0030, 0x0063, 0x0066, 0x00cf, 0x006c, 0x00db, 0x00de, 0x01bf,
+    0x0078, 0x00f3, 0x00f6, 0x01ef, 0x00fc, 0x01fb, 0x01fe, 0x03ff, 0x0060, 0x00c3, 0x00c6, 0x018f,
+    0x00cc, 0x019b, 0x019e, 0x033f, 0x00d8, 0x01b3, 0x01b6, 0x036f, 0x01bc, 0x037b, 0x037e, 0x06ff,
+    0x00f0, 0x01e3, 0x01e6, 0x03cf, 0x01ec, 0x03db, 0x03de, 0x07bf, 0x01f8, 0x03f3, 0x03f6, 0x07ef,
+    0x03fc, 0x07fb, 0x07fe, 0x0fff, 0x00c0, 0x0183, 0x0186, 0x030f, 0x018c, 0x031b, 0x031e, 0x063f,
+    0x0198, 0x0333, 0x0336, 0x066f, 0x033c, 0x067b, 0x067e, 0x0cff, 0x01b0, 0x0363, 0x0366, 0x06cf,
+    0x036c, 0x06db, 0x06de, 0x0dbf, 0x0378, 0x06f3, 0x06f6, 0x0def, 0x06fc, 0x0dfb, 0x0dfe, 0x1bff,
+    0x01e0, 0x03c3, 0x03c6, 0x078f, 0x03cc, 0x079b, 0x079e, 0x0f3f, 0x03d8, 0x07b3, 0x07b6, 0x0f6f,
+    0x07bc, 0x0f7b, 0x0f7e, 0x1eff, 0x03f0, 0x07e3, 0x07e6, 0x0fcf, 0x07ec, 0x0fdb, 0x0fde, 0x1fbf,
+    0x07f8, 0x0ff3, 0x0ff6, 0x1fef, 0x0ffc, 0x1ffb, 0x1ffe, 0x3fff, 0x0180, 0x0303, 0x0306, 0x060f,
+    0x030c, 0x061b, 0x061e, 0x0c3f, 0x0318, 0x0633, 0x0636, 0x0c6f, 0x063c, 0x0c7b, 0x0c7e, 0x18ff,
+    0x0330, 0x0663, 0x0666, 0x0ccf, 0x066c, 0x0cdb, 0x0cde, 0x19bf, 0x0678, 0x0cf3, 0x0cf6, 0x19ef,
+    0x0cfc, 0x19fb, 0x19fe, 0x33ff, 0x0360, 0x06c3, 0x06c6, 0x0d8f, 0x06cc, 0x0d9b, 0x0d9e, 0x1b3f,
+    0x06d8, 0x0db3, 0x0db6, 0x1b6f, 0x0dbc, 0x1b7b, 0x1b7e, 0x36ff, 0x06f0, 0x0de3, 0x0de6, 0x1bcf,
+    0x0dec, 0x1bdb, 0x1bde, 0x37bf, 0x0df8, 0x1bf3, 0x1bf6, 0x37ef, 0x1bfc, 0x37fb, 0x37fe, 0x6fff,
+    0x03c0, 0x0783, 0x0786, 0x0f0f, 0x078c, 0x0f1b, 0x0f1e, 0x1e3f, 0x0798, 0x0f33, 0x0f36, 0x1e6f,
+    0x0f3c, 0x1e7b, 0x1e7e, 0x3cff, 0x07b0, 0x0f63, 0x0f66, 0x1ecf, 0x0f6c, 0x1edb, 0x1ede, 0x3dbf,
+    0x0f78, 0x1ef3, 0x1ef6, 0x3def, 0x1efc, 0x3dfb, 0x3dfe, 0x7bff, 0x07e0, 0x0fc3, 0x0fc6, 0x1f8f,
+    0x0fcc, 0x1f9b, 0x1f9e, 0x3f3f, 0x0fd8, 0x1fb3, 0x1fb6, 0x3f6f, 0x1fbc, 0x3f7b, 0x3f7e, 0x7eff,
+    0x0ff0, 0x1fe3, 0x1fe6, 0x3fcf, 0x1fec, 0x3fdb, 0x3fde, 0x7fbf, 0x1ff8, 0x3ff3, 0x3ff6, 0x7fef,
+    0x3ffc, 0x7ffb, 0x7ffe, 0xffff};
+
+// The bits of y with every one-bit doubled, as a 128-bit value (lo, hi).
+ZFPB_DEV void double_ones(u64 y, u64& lo, u64& hi) {
+  lo = 0;
+  hi = 0;
+  u32 r = 0;  // one-bits below the current byte
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const u32 b = (u32)(y >> (8 * i)) & 0xffu;
+    const u64 t = __ldg(kOnesDoubled + b);
+    const u32 sh = 8 * i + r;  // at most 112
+    if (sh < 64) {
+      lo |= t << sh;
+      if (sh > 48) hi |= t >> (64 - sh);
+    } else {
+      hi |= t << (sh - 64);
+    }
+    r += __popc(b);
+  }
+}
+
+// encode_ints (bitplane.rs:509-610) one bit plane at a time.  A plane with
+// n significant coefficients is coded as its low n bits verbatim followed by
+// the group tests of the rest, y = x >> n.  That code is "0" when y == 0, and
+// otherwise "1" followed by y's bits up to its highest one with every one-bit
+// doubled, the highest one written "10"; when that one is the last
+// coefficient it is implied and omitted with its marker.  This is bit for bit
+// what the reference's group-test loop writes, so the block's stream is the
+// concatenation of plane codes, cut at the budget.
+template <class U, int N, class Wr>
+ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore ps) {
+  if constexpr (N > 64) {
+    return encode_ints_loop<U, N>(w, maxbits, maxprec, u, ps);
+  } else {
+    constexpr u32 intprec = sizeof(U) * 8;
+    constexpr u32 size = N;
+    const u32 budget = with_maxbits(maxbits, maxprec, size) ? maxbits : 0xffffffffu;
+    const u32 kmin = intprec > maxprec ? intprec - maxprec : 0;
+    U all = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) all |= u[i];
+    u32 top;
+    if constexpr (sizeof(U) == 4) top = 32 - __clz((int)all);
+    else top = 64 - __clzll((long long)all);
+    store_planes<U, N>(u, ps);
+
+    u32 bits = budget;
+    u32 n = 0;
+    u32 tk = top > kmin ? top : kmin;
+    u32 empty = intprec - tk;
+    empty = empty < bits ? empty : bits;
+    w.put_zeros(empty);
+    bits -= empty;
+    u32 k = intprec - empty;
+    while (bits != 0 && k > kmin) {
+      k--;
+      const u64 x = ps.at(k, 0, 1);
+      if (n == size) {
+        const u32 take = size < bits ? size : bits;
+        w.put(x & low_mask(take), take);
+        bits -= take;
+        continue;
+      }
+      const u64 y = x >> n;  // n < size <= 64
+      u64 glo = 0, ghi = 0;
+      u32 glen = 1, nn = n;
+      if (y != 0) {
+        const u32 hb = 63 - (u32)__clzll((long long)y);
+        const u32 c = (u32)__popcll((long long)y);
+        u64 elo, ehi;
+        double_ones(y, elo, ehi);
+        const u32 p = hb + c;  // second copy of the highest one: written as 0
+        if (p < 64) elo &= ~(1ull << p);
+        else ehi &= ~(1ull << (p - 64));
+        glo = 1ull | (elo << 1);
+        ghi = (ehi << 1) | (elo >> 63);
+        glen = hb + c + 2;
+        if (hb == size - 1 - n) glen -= 2;  // the last coefficient's one is implied
+        nn = n + hb + 1;
+      }
+      const u32 total = n + glen;
+      const u32 take = total < bits ? total : bits;
+      const u32 tv = n < take ? n : take;
+      w.put(x & low_mask(tv), tv);
+      const u32 tg = take - tv;
+      if (tg <= 64) {
+        w.put(glo & low_mask(tg), tg);
+      } else {
+        w.put(glo, 64);
+        w.put(ghi & low_mask(tg - 64), tg - 64);
+      }
+      bits -= take;
+      n = nn;
+    }
+    return budget - bits;
+  }
 }
 
 ZFPB_DEV u32 ctz64(u64 x) { return x ? (u32)__ffsll((long long)x) - 1 : 64u; }

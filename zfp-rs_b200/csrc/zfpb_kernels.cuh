@@ -166,6 +166,7 @@ ZFPB_DEV void scatter_block(T* base, const FieldGeom& f, i64 off, const int* len
   for (int d = 0; d < D; d++) full = full && len[d] == 4;
   if (owner) {
     const int nx = len[0], ny = D > 1 ? len[1] : 1, nz = D > 2 ? len[2] : 1, nw = D > 3 ? len[3] : 1;
+#pragma unroll
     for (int i = 0; i < N; i++) {
       const int x = i & 3, y = (i >> 2) & 3, z = (i >> 4) & 3, w = i >> 6;
       if (x < nx && y < ny && z < nz && w < nw) {
@@ -210,6 +211,10 @@ template <class T, int D> struct KernelShape {
   static constexpr int PREC = Traits<T>::PREC;
   // Shared-memory words of plane storage per thread.
   static constexpr int PLANE_WORDS = PREC * W;
+  // CTAs of 128 threads per SM the register allocation must allow: 4 caps
+  // 32-bit blocks at 128 registers (16 warps per SM), 2 caps 64-bit ones at
+  // 255.  Occupancy hides the latency of the sequential bit-plane coding.
+  static constexpr int MIN_CTAS = sizeof(T) == 4 ? 4 : 2;
 };
 
 // ---------------------------------------------------------------------------
@@ -221,7 +226,7 @@ template <class T, int D> struct KernelShape {
 // into which it merges the bits already in the stream.
 // ---------------------------------------------------------------------------
 template <class T, int D>
-__global__ void __launch_bounds__(128, 1) k_encode_fixed(EncodeFixedArgs a) {
+__global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_encode_fixed(EncodeFixedArgs a) {
   typedef KernelShape<T, D> S;
   extern __shared__ u64 smem[];
   const int tid = threadIdx.x, nthr = blockDim.x;
@@ -265,7 +270,7 @@ __global__ void __launch_bounds__(128, 1) k_encode_fixed(EncodeFixedArgs a) {
 // scratch buffer (slot i at word i * slot_words), its bit length recorded.
 // ---------------------------------------------------------------------------
 template <class T, int D>
-__global__ void __launch_bounds__(128, 1) k_encode_var(EncodeVarArgs a) {
+__global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_encode_var(EncodeVarArgs a) {
   typedef KernelShape<T, D> S;
   extern __shared__ u64 smem[];
   const int tid = threadIdx.x;
@@ -305,7 +310,7 @@ ZFPB_DEV void check_loads(u64 start, u32 read_bits, u32 occupied, u64 len, unsig
 
 // Fixed-size blocks: block i starts at start + i * maxbits (decompress.rs:205-330).
 template <class T, int D>
-__global__ void __launch_bounds__(128, 1) k_decode_fixed(DecodeArgs a) {
+__global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_fixed(DecodeArgs a) {
   typedef KernelShape<T, D> S;
   extern __shared__ u64 smem[];
   const int tid = threadIdx.x;
@@ -328,7 +333,7 @@ __global__ void __launch_bounds__(128, 1) k_decode_fixed(DecodeArgs a) {
 // and check that it ends where the next begins, which makes the offsets
 // exactly those of a serial decode (else FLAG_BAD_INDEX).
 template <class T, int D>
-__global__ void __launch_bounds__(128, 1) k_decode_var(DecodeArgs a) {
+__global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_var(DecodeArgs a) {
   typedef KernelShape<T, D> S;
   extern __shared__ u64 smem[];
   const int tid = threadIdx.x;
