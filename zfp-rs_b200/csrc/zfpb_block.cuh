@@ -556,18 +556,28 @@ template <bool EDGE_ATOMIC> struct Writer {
 
 // Reads from bit `pos` of a stream of `len` words; words past the end read as
 // zero (core.rs:151-157).  Holds the current partial word and the next word.
+// Words [s0, s0 + sn) may be served from a shared-memory copy (`stage`) of
+// the stream, the rest come from global memory.
 struct Reader {
   const u64* src;
   u64 len;
+  const u64* stage;
+  u64 s0, sn;
   u64 word;  // index of the word after `nxt`
   u64 buf;   // unread bits of the current word, `bits` of them
   u64 nxt;   // the following word
   u32 bits;
 
-  ZFPB_DEV u64 load(u64 i) const { return i < len ? __ldg(src + i) : 0ull; }
-  ZFPB_DEV void init(const u64* s, u64 n, u64 pos) {
+  ZFPB_DEV u64 load(u64 i) const {
+    if (i - s0 < sn) return stage[i - s0];
+    return i < len ? __ldg(src + i) : 0ull;
+  }
+  ZFPB_DEV void init(const u64* s, u64 n, u64 pos, const u64* stg = nullptr, u64 stg0 = 0, u64 stgn = 0) {
     src = s;
     len = n;
+    stage = stg;
+    s0 = stg0;
+    sn = stgn;
     u64 w = pos >> 6;
     u32 off = (u32)(pos & 63);
     if (off) {
@@ -609,7 +619,7 @@ struct Reader {
   // Skip n bits (n may exceed 64).
   ZFPB_DEV void skip(u64 n) {
     u64 p = pos() + n;
-    init(src, len, p);
+    init(src, len, p, stage, s0, sn);
   }
 };
 
@@ -955,6 +965,245 @@ ZFPB_DEV PlaneResult decode_planes(Reader& r, u32 budget, u32 kmin, u32 intprec,
   return res;
 }
 
+// ---------------------------------------------------------------------------
+// Plane-at-a-time decoder for blocks of up to 64 values.
+//
+// decode_planes follows the reference loop, one group test per iteration, so
+// the 32 blocks of a warp run through different branches and the warp issues
+// the union of their paths.  This decoder does the same work in one iteration
+// per bit plane with a bounded amount of work per plane, so that the threads of
+// a warp stay together.  Facts it rests on (the code written by
+// bitplane.rs:509-620 and read by bitplane.rs:675-790):
+//
+// * A plane is n verbatim bits (n = coefficients already significant) and then
+//   the group-test code of the rest.  That code is a GT bit; while it is 1, a
+//   run of zeros ended by a 1 (the next significant coefficient); then the next
+//   GT bit.  So, past the verbatim bits, the code is "1 0^z1 1 1 0^z2 1 ... 0":
+//   its ones pair up as (GT, coefficient), and a bit is a GT bit exactly when
+//   the number of ones up to and including it is odd (a prefix XOR).
+// * The code ends at the first group start holding a 0 (a group start is bit 0
+//   or the bit after a coefficient one), or, once the scan reaches the last
+//   coefficient, without its "1" (the one is implied), or where the budget
+//   runs out.
+// * A plane takes at most 2 * size - n - 1 bits, so a 128-bit window at its
+//   start holds all of it.
+// ---------------------------------------------------------------------------
+
+ZFPB_DEV u64 prefix_xor64(u64 x) {
+  x ^= x << 1;
+  x ^= x << 2;
+  x ^= x << 4;
+  x ^= x << 8;
+  x ^= x << 16;
+  x ^= x << 32;
+  return x;
+}
+
+ZFPB_DEV u32 popc64(u64 x) { return (u32)__popcll((long long)x); }
+
+// Bits of (hi:lo) below position e, e in [0, 128].
+ZFPB_DEV u32 popc_below128(u64 lo, u64 hi, u32 e) {
+  u32 c = popc64(lo & low_mask(e < 64 ? e : 64));
+  if (e > 64) c += popc64(hi & low_mask(e - 64));
+  return c;
+}
+
+ZFPB_DEV u32 bit128(u64 lo, u64 hi, u32 i) { return (u32)((i < 64 ? lo >> i : hi >> (i & 63)) & 1); }
+
+// Position of the r-th (from 0) set bit of x, which has more than r set bits.
+ZFPB_DEV u32 select64(u64 x, u32 r) {
+  u32 pos = 0, c;
+#pragma unroll
+  for (int w = 32; w >= 2; w >>= 1) {
+    c = popc64(x & low_mask((u32)w));
+    if (r >= c) {
+      r -= c;
+      x >>= w;
+      pos += (u32)w;
+    }
+  }
+  c = (u32)(x & 1);
+  return r >= c ? pos + 1 : pos;
+}
+
+ZFPB_DEV u32 select128(u64 lo, u64 hi, u32 r) {
+  const u32 c = popc64(lo);
+  return r < c ? select64(lo, r) : 64 + select64(hi, r - c);
+}
+
+// Three consecutive stream words and a bit offset into the first: a window
+// of 128 bits at the cursor.
+struct Window {
+  const Reader* rd;
+  u64 w0, w1, w2, next;
+  u32 off;
+
+  ZFPB_DEV void init(const Reader* r, u64 pos) {
+    rd = r;
+    const u64 wi = pos >> 6;
+    off = (u32)(pos & 63);
+    w0 = r->load(wi);
+    w1 = r->load(wi + 1);
+    w2 = r->load(wi + 2);
+    next = wi + 3;
+  }
+  ZFPB_DEV u64 lo() const { return (w0 >> off) | ((w1 << 1) << (63 - off)); }
+  ZFPB_DEV u64 hi() const { return (w1 >> off) | ((w2 << 1) << (63 - off)); }
+  ZFPB_DEV void advance(u32 n) {  // n <= 128
+    off += n;
+    if (off >= 64) {
+      w0 = w1;
+      w1 = w2;
+      w2 = rd->load(next++);
+      off -= 64;
+    }
+    if (off >= 64) {
+      w0 = w1;
+      w1 = w2;
+      w2 = rd->load(next++);
+      off -= 64;
+    }
+  }
+  ZFPB_DEV u64 pos() const { return ((next - 3) << 6) + off; }
+};
+
+// Same contract and results as decode_planes, for N <= 64.
+template <int N>
+ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 intprec, PlaneStore ps) {
+  static_assert(N <= 64, "one plane word per plane");
+  constexpr u32 size = N;
+  constexpr bool WIDE = N == 64;  // the window needs its second word
+  Window r;
+  r.init(&rd, rd.pos());
+  u32 bits = budget, n = 0, m = 0, k = intprec;
+  int low = (int)intprec, high = -1;
+  while (bits != 0) {
+    m = 0;
+    if (k <= kmin) {
+      k = k - 1;
+      break;
+    }
+    const u64 lo = r.lo();
+    if (n == 0) {
+      // Leading empty planes: one 0 bit each (bitplane.rs:700-712).
+      u32 e = ctz64(lo);
+      e = e < k - kmin ? e : k - kmin;
+      e = e < bits ? e : bits;
+      if (e != 0) {
+        r.advance(e);
+        bits -= e;
+        k -= e;
+        m = size;
+        continue;
+      }
+    }
+    k--;
+    u64 x;
+    u32 used;
+    if (n == size) {
+      // Every coefficient significant: the plane is verbatim.
+      used = bits > size ? size : bits;
+      x = lo & low_mask(used);
+      m = bits > size ? 0 : bits;
+      bits -= used;
+    } else {
+      used = n < bits ? n : bits;
+      x = lo & low_mask(used);
+      m = used;
+      bits -= used;
+      if (bits != 0) {
+        const u64 hi = WIDE ? r.hi() : 0ull;
+        // The group-test code, from bit n of the window.
+        const u64 t0 = n ? (lo >> n) | (hi << (64 - n)) : lo;
+        const u64 t1 = n ? hi >> n : hi;
+        if ((t0 & 1) == 0) {
+          used += 1;
+          bits -= 1;
+          m = size;
+        } else {
+          const u64 p0 = prefix_xor64(t0);
+          const u64 p1 = WIDE ? prefix_xor64(t1) ^ (0ull - (p0 >> 63)) : 0ull;
+          const u64 s0 = t0 & ~p0, s1 = t1 & ~p1;  // coefficient ones
+          const u64 g0 = t0 & p0, g1 = t1 & p1;    // GT ones
+          const u64 b0 = (s0 << 1) | 1, b1 = (s1 << 1) | (s0 >> 63);  // group starts
+          const u32 e = WIDE ? (((b0 & ~t0) != 0) ? ctz64(b0 & ~t0) : 64 + ctz64(b1 & ~t1)) : ctz64(b0 & ~t0);
+          const u32 lim = WIDE ? 128 : 64;
+          const u32 ce = n + e - popc_below128(g0, g1, e);  // coefficients read before bit e
+          const bool regular = e < lim && ce <= size - 1;
+          const u32 a = bits;  // budget left for the code
+          u32 end, extra = 64, n_new, m_new;
+          if (regular && e < a) {
+            end = e + 1;
+            n_new = ce;
+            m_new = size;
+          } else {
+            // Ended by the implied last one (not a terminator), or cut by the budget.
+            u32 istar = lim;
+            u32 bs = 0;
+            if (!regular) {
+              const u32 L = size - 1 - n;  // coefficient zeros before the implied one
+              istar = L == 0 ? 0 : select128(~g0, WIDE ? ~g1 : 0ull, L - 1) + 1;
+              bs = bit128(b0, b1, istar < lim ? istar : 0);
+            }
+            if (!regular && (bs ? istar < a : istar <= a)) {
+              end = istar + bs;
+              extra = size - 1 - n;
+              n_new = size;
+              m_new = size;
+            } else {
+              end = a;  // a < lim here
+              const u32 ca = n + a - popc_below128(g0, g1, a);
+              if (bit128(b0, b1, a)) {
+                n_new = ca;
+              } else {
+                extra = ca - n;  // the reader's implied one at the cut
+                n_new = ca + 1;
+              }
+              m_new = n_new;
+            }
+          }
+          // Coefficient ones before `end`, each moved down past the GT bits
+          // before it: the j-th (from 1) at bit s goes to coefficient s - j.
+          u64 q0 = s0 & low_mask(end < 64 ? end : 64);
+          u64 q1 = (WIDE && end > 64) ? s1 & low_mask(end - 64) : 0ull;
+          u64 y = extra < 64 ? 1ull << extra : 0ull;
+          u32 j = 1;
+          while (q0) {
+            y |= 1ull << (ctz64(q0) - j);
+            j++;
+            q0 &= q0 - 1;
+          }
+          if (WIDE) {
+            while (q1) {
+              y |= 1ull << (64 + ctz64(q1) - j);
+              j++;
+              q1 &= q1 - 1;
+            }
+          }
+          x |= y << n;
+          used += end;
+          bits -= end;
+          n = n_new;
+          m = m_new;
+        }
+      }
+    }
+    r.advance(used);
+    ps.at(k, 0, 1) = x;
+    if (high < 0) high = (int)k;
+    low = (int)k;
+  }
+  if (n == 0) low = (int)intprec;
+  rd.init(rd.src, rd.len, r.pos(), rd.stage, rd.s0, rd.sn);
+  PlaneResult res;
+  res.bits = budget - bits;
+  res.m = m;
+  res.prec = intprec - k;
+  res.low = low;
+  res.high = high;
+  return res;
+}
+
 // decode_ints (bitplane.rs:626-667) into u; returns bits read, sets *zero.
 template <class U, int N>
 ZFPB_DEV u32 decode_ints(Reader& r, u32 maxbits, u32 maxprec, int rounding, U* u, bool* zero,
@@ -963,7 +1212,9 @@ ZFPB_DEV u32 decode_ints(Reader& r, u32 maxbits, u32 maxprec, int rounding, U* u
   const bool constrained = with_maxbits(maxbits, maxprec, N);
   const u32 budget = constrained ? maxbits : 0xffffffffu;
   const u32 kmin = intprec > maxprec ? intprec - maxprec : 0;
-  PlaneResult pr = decode_planes<N>(r, budget, kmin, intprec, ps);
+  PlaneResult pr;
+  if constexpr (N <= 64) pr = decode_planes_sync<N>(r, budget, kmin, intprec, ps);
+  else pr = decode_planes<N>(r, budget, kmin, intprec, ps);
   bool z = pr.low == (int)intprec;
   if (z) {
 #pragma unroll

@@ -64,6 +64,7 @@ struct DecodeArgs {
   // result is that of a serial decode (zfp-rs decompress.rs:153-186).
   u64* owner;
   i64 imin;
+  u64 stage_words;  // shared-memory words for the CTA's stream segment
 };
 
 // Whether two index tuples of the field can address the same element

@@ -36,18 +36,27 @@ template <class T, int D> static cudaError_t encode_var_d(const EncodeVarArgs& a
   return cudaGetLastError();
 }
 
-template <class T, int D> static cudaError_t decode_fixed_d(const DecodeArgs& a, cudaStream_t s) {
+// Shared-memory words for a decoding CTA's stream segment: 16 KiB for 32-bit
+// types (4 CTAs of 48 KiB per SM), 32 KiB for 64-bit ones (2 of 96 KiB);
+// a longer segment reads its tail from global memory.
+template <class T, int D> static u64 stage_words() { return sizeof(T) == 4 ? 2048 : 4096; }
+
+template <class T, int D> static cudaError_t decode_fixed_d(const DecodeArgs& a0, cudaStream_t s) {
   const int th = var_threads<T, D>();
-  size_t smem = plane_smem<T, D>(th);
+  DecodeArgs a = a0;
+  a.stage_words = stage_words<T, D>();
+  size_t smem = plane_smem<T, D>(th) + a.stage_words * sizeof(u64);
   cudaError_t e = set_smem<T, D>((const void*)k_decode_fixed<T, D>, smem);
   if (e != cudaSuccess) return e;
   k_decode_fixed<T, D><<<grid_of(a.f.nblocks, th), th, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-template <class T, int D> static cudaError_t decode_var_d(const DecodeArgs& a, cudaStream_t s) {
+template <class T, int D> static cudaError_t decode_var_d(const DecodeArgs& a0, cudaStream_t s) {
   const int th = var_threads<T, D>();
-  size_t smem = plane_smem<T, D>(th);
+  DecodeArgs a = a0;
+  a.stage_words = stage_words<T, D>();
+  size_t smem = plane_smem<T, D>(th) + a.stage_words * sizeof(u64);
   cudaError_t e = set_smem<T, D>((const void*)k_decode_var<T, D>, smem);
   if (e != cudaSuccess) return e;
   k_decode_var<T, D><<<grid_of(a.f.nblocks, th), th, smem, s>>>(a);
