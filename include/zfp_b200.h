@@ -82,7 +82,8 @@ size_t zfpb_compress_device_noalloc(const zfpb_desc* desc, const void* d_field, 
  * clears the totals.  zfpb_timing_read fills, per kernel kind, the summed
  * milliseconds and the launch count, and returns the number of kinds:
  * 0 encode_fixed, 1 encode_var, 2 scan, 3 pack, 4 decode_fixed,
- * 5 decode_var, 6 walk, 7 claim, 8 offsets. */
+ * 5 decode_var, 6 walk, 7 claim, 8 offsets, 9 parse, 10 finish (the two
+ * halves of the decoder used for 3D fields). */
 void zfpb_timing_enable(int on);
 int zfpb_timing_read(double* ms, unsigned long long* counts, int n);
 

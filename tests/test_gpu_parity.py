@@ -248,3 +248,44 @@ def test_device_resident_zfp_field_and_stream():
         L.zfp_field_free(p)
     L.zfp_stream_close(zs)
     L.stream_close(bs)
+
+
+def spiky(n, dtype, seed):
+    """A bench-like field: smooth x1e3 + noise, 10% zero blocks, 1% spikes."""
+    rng = np.random.default_rng(seed)
+    x = np.arange(n, dtype=np.float64)
+    f = np.sin(0.10 * x)[None, None, :] * np.cos(0.13 * x)[None, :, None] * np.sin(0.07 * x)[:, None, None]
+    f = (f + rng.normal(0, 1e-3, size=(n, n, n))) * 1e3
+    nb = n // 4
+    zero = rng.random((nb, nb, nb)) < 0.10
+    f.reshape(nb, 4, nb, 4, nb, 4)[zero[:, None, :, None, :, None].repeat(4, 1).repeat(4, 3).repeat(4, 5)] = 0.0
+    spikes = rng.random(f.shape) < 0.01
+    k = int(spikes.sum())
+    f[spikes] = rng.choice([-1.0, 1.0], size=k) * 10.0 ** rng.uniform(-30, 30, size=k)
+    return f.astype(dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64], ids=lambda d: np.dtype(d).name)
+def test_spiky_field_many_blocks_matches_oracle(dtype):
+    arr = spiky(48, dtype, seed=4)
+    for cfg in [Z.ZfpConfig.fixed_accuracy(1e-6), Z.ZfpConfig.fixed_precision(32).with_rounding("last", True),
+                Z.ZfpConfig.fixed_rate(8, dtype, 3), Z.ZfpConfig.fixed_rate(21, dtype, 3).with_rounding("last"),
+                Z.ZfpConfig.reversible()]:
+        check(arr, cfg)
+
+
+@pytest.mark.parametrize("dtype", DTYPES, ids=lambda d: np.dtype(d).name)
+def test_one_kernel_decoder_matches_two_kernel_decoder(dtype, monkeypatch):
+    """3D fields decode with k_parse + k_finish; ZFPB_ONE_KERNEL_DECODE=1
+    selects the one-kernel decoder (used for other dimensions and when the
+    plane scratch cannot be allocated).  Both must give the oracle's values."""
+    arr = spiky(24, dtype, seed=8) if np.dtype(dtype).kind == "f" else smooth((24, 20, 16), dtype, seed=8)
+    cfgs = [Z.ZfpConfig.fixed_rate(7, dtype, 3), Z.ZfpConfig.fixed_precision(24).with_rounding("last"),
+            Z.ZfpConfig.reversible(), Z.ZfpConfig.expert(30, 900, 40, -60)]
+    if np.dtype(dtype).kind == "f":
+        cfgs.append(Z.ZfpConfig.fixed_accuracy(1e-5).with_rounding("first", True))
+    for cfg in cfgs:
+        monkeypatch.setenv("ZFPB_ONE_KERNEL_DECODE", "1")
+        a = check(arr, cfg)
+        monkeypatch.delenv("ZFPB_ONE_KERNEL_DECODE")
+        assert check(arr, cfg) == a

@@ -556,28 +556,18 @@ template <bool EDGE_ATOMIC> struct Writer {
 
 // Reads from bit `pos` of a stream of `len` words; words past the end read as
 // zero (core.rs:151-157).  Holds the current partial word and the next word.
-// Words [s0, s0 + sn) may be served from a shared-memory copy (`stage`) of
-// the stream, the rest come from global memory.
 struct Reader {
   const u64* src;
   u64 len;
-  const u64* stage;
-  u64 s0, sn;
   u64 word;  // index of the word after `nxt`
   u64 buf;   // unread bits of the current word, `bits` of them
   u64 nxt;   // the following word
   u32 bits;
 
-  ZFPB_DEV u64 load(u64 i) const {
-    if (i - s0 < sn) return stage[i - s0];
-    return i < len ? __ldg(src + i) : 0ull;
-  }
-  ZFPB_DEV void init(const u64* s, u64 n, u64 pos, const u64* stg = nullptr, u64 stg0 = 0, u64 stgn = 0) {
+  ZFPB_DEV u64 load(u64 i) const { return i < len ? __ldg(src + i) : 0ull; }
+  ZFPB_DEV void init(const u64* s, u64 n, u64 pos) {
     src = s;
     len = n;
-    stage = stg;
-    s0 = stg0;
-    sn = stgn;
     u64 w = pos >> 6;
     u32 off = (u32)(pos & 63);
     if (off) {
@@ -619,7 +609,7 @@ struct Reader {
   // Skip n bits (n may exceed 64).
   ZFPB_DEV void skip(u64 n) {
     u64 p = pos() + n;
-    init(src, len, p, stage, s0, sn);
+    init(src, len, p);
   }
 };
 
@@ -1194,7 +1184,7 @@ ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 in
     low = (int)k;
   }
   if (n == 0) low = (int)intprec;
-  rd.init(rd.src, rd.len, r.pos(), rd.stage, rd.s0, rd.sn);
+  rd.init(rd.src, rd.len, r.pos());
   PlaneResult res;
   res.bits = budget - bits;
   res.m = m;
@@ -1456,6 +1446,186 @@ ZFPB_DEV u32 decode_block(Reader& r, T* blk, const Codec& c, PlaneStore ps, u32*
     bits = decode_int_block<I, N>(r, c.maxbits, c.maxprec, c.rounding, blk, ps);
     *read_bits = bits;
     return bits < c.minbits ? c.minbits : bits;
+  }
+}
+
+// ---- two-kernel decoding ----------------------------------------------------
+//
+// The same decode as decode_block, cut in two: parse_block reads a block's
+// bits (header and bit planes; the planes go to the plane store, which here is
+// a plane-major scratch in global memory) and returns a BlockHead;
+// finish_block turns the head and the planes into values.  The head carries
+// the block's kind, its exponent and the decode_ints state the value half
+// needs (bitplane.rs:626-667), packed into one word between the kernels.
+
+enum : u32 { HEAD_ZERO = 0, HEAD_FLOAT = 1, HEAD_INT = 2, HEAD_REV_REINTERP = 3, HEAD_REV_FLOAT = 4, HEAD_REV_INT = 5 };
+
+struct BlockHead {
+  u32 kind;
+  int emax;
+  int low, high;  // stored planes [low, high]; low = intprec if none
+  u32 m, prec;    // inverse-rounding arguments
+  bool round;     // ROUND_LAST
+  bool z;         // no plane stored
+
+  // kind 3 bits, emax + 2048 12 bits, low 9, high + 1 9, m 9, prec 8, round, z.
+  ZFPB_DEV u64 pack() const {
+    return (u64)kind | ((u64)(u32)(emax + 2048) & 0xfff) << 3 | (u64)((u32)low & 0x1ff) << 15 |
+           (u64)((u32)(high + 1) & 0x1ff) << 24 | (u64)(m & 0x1ff) << 33 | (u64)(prec & 0xff) << 42 |
+           (u64)round << 50 | (u64)z << 51;
+  }
+  ZFPB_DEV static BlockHead unpack(u64 v) {
+    BlockHead h;
+    h.kind = (u32)(v & 7);
+    h.emax = (int)((v >> 3) & 0xfff) - 2048;
+    h.low = (int)((v >> 15) & 0x1ff);
+    h.high = (int)((v >> 24) & 0x1ff) - 1;
+    h.m = (u32)((v >> 33) & 0x1ff);
+    h.prec = (u32)((v >> 42) & 0xff);
+    h.round = (v >> 50) & 1;
+    h.z = (v >> 51) & 1;
+    return h;
+  }
+};
+
+// decode_ints, stream half: read the planes into ps; returns bits read.
+template <class U, int N>
+ZFPB_DEV u32 parse_ints(Reader& r, u32 maxbits, u32 maxprec, int rounding, PlaneStore ps, BlockHead& h) {
+  constexpr u32 intprec = sizeof(U) * 8;
+  const bool constrained = with_maxbits(maxbits, maxprec, N);
+  const u32 budget = constrained ? maxbits : 0xffffffffu;
+  const u32 kmin = intprec > maxprec ? intprec - maxprec : 0;
+  PlaneResult pr;
+  if constexpr (N <= 64) pr = decode_planes_sync<N>(r, budget, kmin, intprec, ps);
+  else pr = decode_planes<N>(r, budget, kmin, intprec, ps);
+  h.low = pr.low;
+  h.high = pr.high;
+  h.z = pr.low == (int)intprec;
+  h.round = rounding == 2;
+  h.m = pr.m;
+  h.prec = pr.prec;
+  if (!constrained) {
+    h.m = 0;
+    h.prec = intprec - (kmin - 1);
+  }
+  return pr.bits;
+}
+
+// decode_ints, value half: planes -> coefficients, inverse rounding, then the
+// inverse reorder and transform (decode/core.rs:97-131, KIND 1;
+// decode/reversible.rs:46-82, KIND 3).
+template <class I, int N, int KIND>
+ZFPB_DEV void finish_int_block(const BlockHead& h, I* ib, PlaneStore ps) {
+  typedef typename Traits<I>::U U;
+  U u[N];
+  if (h.z) {
+#pragma unroll
+    for (int i = 0; i < N; i++) u[i] = 0;
+  } else {
+    load_planes<U, N>(u, ps, h.low, h.high);
+  }
+  if (h.round) inv_round<U, N>(u, h.m, h.prec);
+  if (KIND == 1 && h.z && !h.round) {
+#pragma unroll
+    for (int i = 0; i < N; i++) ib[i] = 0;
+  } else {
+    inv_order<N>(u, ib);
+    inv_axes<I, N, KIND>(ib);
+  }
+}
+
+// decode/reversible.rs:46-82, stream half.
+template <class U, int N>
+ZFPB_DEV u32 parse_rev_int_block(Reader& r, u32 maxbits, PlaneStore ps, BlockHead& h) {
+  constexpr u32 PB = sizeof(U) == 4 ? 5 : 6;
+  u32 prec = (u32)r.read(PB) + 1;
+  return PB + parse_ints<U, N>(r, sat_sub(maxbits, PB), prec, 0, ps, h);
+}
+
+// Stream half of decode_block: returns the bits the block occupies (after the
+// skip to minbits) and, in *read_bits, the bits actually read.
+template <class T, int N>
+ZFPB_DEV u32 parse_block(Reader& r, const Codec& c, PlaneStore ps, BlockHead& h, u32* read_bits) {
+  typedef typename Traits<T>::U U;
+  h.emax = 0;
+  h.low = h.high = 0;
+  h.m = h.prec = 0;
+  h.round = h.z = false;
+  u32 bits;
+  if (c.minexp < ZFP_MIN_EXP) {
+    if constexpr (!Traits<T>::FLOAT) {
+      h.kind = HEAD_REV_INT;
+      bits = parse_rev_int_block<U, N>(r, c.maxbits, ps, h);
+    } else {
+      if (r.read_bit() == 0) {
+        h.kind = HEAD_ZERO;
+        bits = 1;
+      } else {
+        bits = 2;
+        if (r.read_bit()) {
+          h.kind = HEAD_REV_REINTERP;
+          bits += parse_rev_int_block<U, N>(r, sat_sub(c.maxbits, bits), ps, h);
+        } else {
+          h.kind = HEAD_REV_FLOAT;
+          h.emax = (int)r.read(Traits<T>::EBITS) - Traits<T>::EBIAS;
+          bits += Traits<T>::EBITS;
+          bits += parse_rev_int_block<U, N>(r, sat_sub(c.maxbits, bits), ps, h);
+        }
+      }
+    }
+    *read_bits = bits;
+    return bits < c.minbits ? c.minbits : bits;
+  }
+  if constexpr (Traits<T>::FLOAT) {
+    if (r.read_bit()) {
+      constexpr u32 hb = 1 + Traits<T>::EBITS;
+      h.kind = HEAD_FLOAT;
+      h.emax = (int)r.read(Traits<T>::EBITS) - Traits<T>::EBIAS;
+      u32 prec = precision_f(h.emax, c.maxprec, c.minexp, Dims<N>::value, c.tight != 0);
+      u32 ibits = parse_ints<U, N>(r, sat_sub(c.maxbits, hb), prec, c.rounding, ps, h);
+      u32 mb = sat_sub(c.minbits, hb);
+      *read_bits = hb + ibits;
+      return hb + (ibits < mb ? mb : ibits);
+    }
+    h.kind = HEAD_ZERO;
+    *read_bits = 1;
+    return c.minbits > 1 ? c.minbits : 1;
+  } else {
+    h.kind = HEAD_INT;
+    bits = parse_ints<U, N>(r, c.maxbits, c.maxprec, c.rounding, ps, h);
+    *read_bits = bits;
+    return bits < c.minbits ? c.minbits : bits;
+  }
+}
+
+// Value half of decode_block.
+template <class T, int N>
+ZFPB_DEV void finish_block(const BlockHead& h, T* blk, PlaneStore ps) {
+  typedef typename Traits<T>::I I;
+  typedef typename Traits<T>::U U;
+  if constexpr (!Traits<T>::FLOAT) {
+    if (h.kind == HEAD_REV_INT) finish_int_block<I, N, 3>(h, reinterpret_cast<I*>(blk), ps);
+    else finish_int_block<I, N, 1>(h, reinterpret_cast<I*>(blk), ps);
+  } else {
+    if (h.kind == HEAD_ZERO) {
+#pragma unroll
+      for (int i = 0; i < N; i++) blk[i] = 0;
+      return;
+    }
+    I ib[N];
+    if (h.kind == HEAD_FLOAT) {
+      finish_int_block<I, N, 1>(h, ib, ps);
+      inv_cast<T, N>(ib, blk, h.emax);
+    } else {
+      finish_int_block<I, N, 3>(h, ib, ps);
+      if (h.kind == HEAD_REV_REINTERP) {
+        const U tc = (U)(~(U)0) >> 1;
+#pragma unroll
+        for (int i = 0; i < N; i++) blk[i] = float_of(ib[i] < 0 ? (U)((U)ib[i] ^ tc) : (U)ib[i]);
+      } else {
+        inv_cast<T, N>(ib, blk, h.emax);
+      }
+    }
   }
 }
 

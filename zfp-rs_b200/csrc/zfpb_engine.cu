@@ -5,6 +5,7 @@
 // src/decompress.rs.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -84,7 +85,7 @@ size_t plane_bytes(int type, int dims) {
 // ---------------------------------------------------------------------------
 
 enum KernelKind { K_ENCODE_FIXED, K_ENCODE_VAR, K_SCAN, K_PACK, K_DECODE_FIXED, K_DECODE_VAR, K_WALK, K_CLAIM,
-                  K_OFFSETS, K_COUNT };
+                  K_OFFSETS, K_PARSE, K_FINISH, K_COUNT };
 
 struct PendingTimer {
   int kind;
@@ -322,7 +323,7 @@ struct Buf {
 };
 
 struct Workspace {
-  Buf slots, lengths, offsets, partial, small, owner;
+  Buf slots, lengths, offsets, partial, small, owner, planes, heads;
   u64* h_pinned = nullptr;  // two words for totals and flags
 };
 
@@ -484,6 +485,45 @@ Status compress(const Call& call, const void* d_field, u64* d_out, u64 cap, u64 
   return OK;
 }
 
+// Decode every block, from i * maxbits (var false) or from a.offsets (var
+// true).  3D fields use the two-kernel decoder (k_parse, k_finish), whose
+// plane scratch is as large as the field.  Other fields, 3D fields whose
+// scratch cannot be had, and every field while the environment variable
+// ZFPB_ONE_KERNEL_DECODE is 1 use the one-kernel decoder.  Both give the
+// same values.
+static cudaError_t decode_blocks(Workspace& ws, const Call& call, const DecodeArgs& a, bool var, cudaStream_t s) {
+  const u64 n = call.f.nblocks;
+  const char* one = getenv("ZFPB_ONE_KERNEL_DECODE");
+  if (call.dims == 3 && !(one && one[0] == '1')) {
+    const u64 stride = (n + 31) & ~31ull;
+    const u64 planes = (call.type == 1 || call.type == 3) ? 32 : 64;
+    if (stride < (1ull << 31) && ws.planes.ensure(planes * stride * sizeof(u64)) == cudaSuccess &&
+        ws.heads.ensure(n * sizeof(u64)) == cudaSuccess) {
+      SplitArgs sa{(u64*)ws.planes.p, stride, (u64*)ws.heads.p};
+      cudaError_t e;
+      {
+        KernelTimer t(K_PARSE, s);
+        e = for_type(call.type, [&](auto* tp) {
+          using T = std::remove_pointer_t<decltype(tp)>;
+          return Launch<T>::parse(call, a, sa, var, s);
+        });
+      }
+      if (e != cudaSuccess) return e;
+      KernelTimer t(K_FINISH, s);
+      return for_type(call.type, [&](auto* tp) {
+        using T = std::remove_pointer_t<decltype(tp)>;
+        return Launch<T>::finish(call, a, sa, s);
+      });
+    }
+    cudaGetLastError();  // a failed scratch allocation: use the one-kernel decoder
+  }
+  KernelTimer t(var ? K_DECODE_VAR : K_DECODE_FIXED, s);
+  return for_type(call.type, [&](auto* tp) {
+    using T = std::remove_pointer_t<decltype(tp)>;
+    return var ? Launch<T>::decode_var(call, a, s) : Launch<T>::decode_fixed(call, a, s);
+  });
+}
+
 Status decompress(const Call& call, const u64* d_in, u64 len, u64 start, void* d_field, u64* end_bit,
                   const u64* d_offsets, cudaStream_t s) {
   std::lock_guard<std::mutex> lock(g_mu);
@@ -526,13 +566,7 @@ Status decompress(const Call& call, const u64* d_in, u64 len, u64 start, void* d
     ZFPB_CHECK(cudaGetLastError());
   }
   if (fixed_size_blocks(call)) {
-    {
-      KernelTimer t(K_DECODE_FIXED, s);
-      ZFPB_CHECK(for_type(call.type, [&](auto* tp) {
-        using T = std::remove_pointer_t<decltype(tp)>;
-        return Launch<T>::decode_fixed(call, a, s);
-      }));
-    }
+    ZFPB_CHECK(decode_blocks(ws, call, a, false, s));
     ZFPB_CHECK(cudaMemcpyAsync(ws.h_pinned, flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     ZFPB_CHECK(cudaStreamSynchronize(s));
     *end_bit = start + n * (u64)call.c.maxbits;
@@ -542,13 +576,7 @@ Status decompress(const Call& call, const u64* d_in, u64 len, u64 start, void* d
   u64* off = nullptr;
   if (d_offsets) {
     a.offsets = const_cast<u64*>(d_offsets);
-    {
-      KernelTimer t(K_DECODE_VAR, s);
-      ZFPB_CHECK(for_type(call.type, [&](auto* tp) {
-        using T = std::remove_pointer_t<decltype(tp)>;
-        return Launch<T>::decode_var(call, a, s);
-      }));
-    }
+    ZFPB_CHECK(decode_blocks(ws, call, a, true, s));
     ZFPB_CHECK(cudaMemcpyAsync(ws.h_pinned, flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     ZFPB_CHECK(cudaStreamSynchronize(s));
     fl = *(unsigned*)ws.h_pinned;
@@ -567,13 +595,7 @@ Status decompress(const Call& call, const u64* d_in, u64 len, u64 start, void* d
         return Launch<T>::walk(call, a, s);
       }));
     }
-    {
-      KernelTimer t(K_DECODE_VAR, s);
-      ZFPB_CHECK(for_type(call.type, [&](auto* tp) {
-        using T = std::remove_pointer_t<decltype(tp)>;
-        return Launch<T>::decode_var(call, a, s);
-      }));
-    }
+    ZFPB_CHECK(decode_blocks(ws, call, a, true, s));
     ZFPB_CHECK(cudaMemcpyAsync(ws.h_pinned, flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     ZFPB_CHECK(cudaStreamSynchronize(s));
     fl = *(unsigned*)ws.h_pinned;

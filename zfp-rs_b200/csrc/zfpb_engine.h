@@ -64,7 +64,13 @@ struct DecodeArgs {
   // result is that of a serial decode (zfp-rs decompress.rs:153-186).
   u64* owner;
   i64 imin;
-  u64 stage_words;  // shared-memory words for the CTA's stream segment
+};
+
+// Scratch of the two-kernel decoder: plane k of block i at planes[k * stride + i].
+struct SplitArgs {
+  u64* planes;
+  u64 stride;
+  u64* heads;
 };
 
 // Whether two index tuples of the field can address the same element
@@ -115,6 +121,9 @@ template <class T> struct Launch {
   static cudaError_t decode_fixed(const Call& call, const DecodeArgs& a, cudaStream_t s);
   static cudaError_t decode_var(const Call& call, const DecodeArgs& a, cudaStream_t s);
   static cudaError_t walk(const Call& call, const DecodeArgs& a, cudaStream_t s);
+  // Two-kernel decoder, 3D fields only.
+  static cudaError_t parse(const Call& call, const DecodeArgs& a, const SplitArgs& sa, bool var, cudaStream_t s);
+  static cudaError_t finish(const Call& call, const DecodeArgs& a, const SplitArgs& sa, cudaStream_t s);
 };
 
 // Compress from bit 0 of d_out (cap words) without allocating device memory:

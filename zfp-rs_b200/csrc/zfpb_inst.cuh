@@ -36,27 +36,18 @@ template <class T, int D> static cudaError_t encode_var_d(const EncodeVarArgs& a
   return cudaGetLastError();
 }
 
-// Shared-memory words for a decoding CTA's stream segment: 16 KiB for 32-bit
-// types (4 CTAs of 48 KiB per SM), 32 KiB for 64-bit ones (2 of 96 KiB);
-// a longer segment reads its tail from global memory.
-template <class T, int D> static u64 stage_words() { return sizeof(T) == 4 ? 2048 : 4096; }
-
-template <class T, int D> static cudaError_t decode_fixed_d(const DecodeArgs& a0, cudaStream_t s) {
+template <class T, int D> static cudaError_t decode_fixed_d(const DecodeArgs& a, cudaStream_t s) {
   const int th = var_threads<T, D>();
-  DecodeArgs a = a0;
-  a.stage_words = stage_words<T, D>();
-  size_t smem = plane_smem<T, D>(th) + a.stage_words * sizeof(u64);
+  size_t smem = plane_smem<T, D>(th);
   cudaError_t e = set_smem<T, D>((const void*)k_decode_fixed<T, D>, smem);
   if (e != cudaSuccess) return e;
   k_decode_fixed<T, D><<<grid_of(a.f.nblocks, th), th, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-template <class T, int D> static cudaError_t decode_var_d(const DecodeArgs& a0, cudaStream_t s) {
+template <class T, int D> static cudaError_t decode_var_d(const DecodeArgs& a, cudaStream_t s) {
   const int th = var_threads<T, D>();
-  DecodeArgs a = a0;
-  a.stage_words = stage_words<T, D>();
-  size_t smem = plane_smem<T, D>(th) + a.stage_words * sizeof(u64);
+  size_t smem = plane_smem<T, D>(th);
   cudaError_t e = set_smem<T, D>((const void*)k_decode_var<T, D>, smem);
   if (e != cudaSuccess) return e;
   k_decode_var<T, D><<<grid_of(a.f.nblocks, th), th, smem, s>>>(a);
@@ -90,6 +81,20 @@ template <class T> cudaError_t Launch<T>::decode_fixed(const Call& call, const D
 }
 template <class T> cudaError_t Launch<T>::decode_var(const Call& call, const DecodeArgs& a, cudaStream_t s) {
   ZFPB_DISPATCH(call, decode_var_d, a, s)
+}
+template <class T>
+cudaError_t Launch<T>::parse(const Call& call, const DecodeArgs& a, const SplitArgs& sa, bool var, cudaStream_t s) {
+  if (call.dims != 3) return cudaErrorInvalidValue;
+  const unsigned g = grid_of(a.f.nblocks, 128);
+  if (var) k_parse<T, 3, true><<<g, 128, 0, s>>>(a, sa);
+  else k_parse<T, 3, false><<<g, 128, 0, s>>>(a, sa);
+  return cudaGetLastError();
+}
+template <class T>
+cudaError_t Launch<T>::finish(const Call& call, const DecodeArgs& a, const SplitArgs& sa, cudaStream_t s) {
+  if (call.dims != 3) return cudaErrorInvalidValue;
+  k_finish<T, 3><<<grid_of(a.f.nblocks, 128), 128, 0, s>>>(a, sa);
+  return cudaGetLastError();
 }
 template <class T> cudaError_t Launch<T>::walk(const Call& call, const DecodeArgs& a, cudaStream_t s) {
   ZFPB_DISPATCH(call, walk_d, a, s)

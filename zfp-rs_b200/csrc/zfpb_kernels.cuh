@@ -308,34 +308,18 @@ ZFPB_DEV void check_loads(u64 start, u32 read_bits, u32 occupied, u64 len, unsig
   if (any && last >= len) atomicOr(flags, FLAG_TRUNCATED);
 }
 
-// Copy stream words [w0, w0 + n) (at most `cap`) into shared memory with
-// coalesced loads; words past the stream end read as zero.  Returns how many.
-ZFPB_DEV u64 stage_stream(u64* stage, u64 cap, const u64* src, u64 len, u64 w0, u64 n) {
-  const u64 m = n < cap ? n : cap;
-  for (u64 i = threadIdx.x; i < m; i += blockDim.x) stage[i] = (w0 + i) < len ? __ldg(src + w0 + i) : 0ull;
-  return m;
-}
-
 // Fixed-size blocks: block i starts at start + i * maxbits (decompress.rs:205-330).
-// The CTA's part of the stream is staged in shared memory first.
 template <class T, int D>
 __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_fixed(DecodeArgs a) {
   typedef KernelShape<T, D> S;
   extern __shared__ u64 smem[];
   const int tid = threadIdx.x;
   PlaneStore ps{smem + tid, (int)blockDim.x};
-  u64* stage = smem + (size_t)S::PLANE_WORDS * blockDim.x;
-  const u64 first = (u64)blockIdx.x * blockDim.x;
-  const u64 last = first + blockDim.x < a.f.nblocks ? first + blockDim.x : a.f.nblocks;
-  const u64 b0 = a.start + first * (u64)a.c.maxbits, b1 = a.start + last * (u64)a.c.maxbits;
-  const u64 w0 = b0 >> 6;
-  const u64 sn = stage_stream(stage, a.stage_words, a.stream, a.stream_len, w0, (b1 >> 6) - w0 + 2);
-  __syncthreads();
-  const u64 blk = first + tid;
+  const u64 blk = (u64)blockIdx.x * blockDim.x + tid;
   if (blk >= a.f.nblocks) return;
   const u64 pos = a.start + blk * (u64)a.c.maxbits;
   Reader r;
-  r.init(a.stream, a.stream_len, pos, stage, w0, sn);
+  r.init(a.stream, a.stream_len, pos);
   T b[S::N];
   u32 rb;
   u32 occ = decode_block<T, S::N>(r, b, a.c, ps, &rb);
@@ -354,19 +338,12 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_var
   extern __shared__ u64 smem[];
   const int tid = threadIdx.x;
   PlaneStore ps{smem + tid, (int)blockDim.x};
-  u64* stage = smem + (size_t)S::PLANE_WORDS * blockDim.x;
-  const u64 first = (u64)blockIdx.x * blockDim.x;
-  const u64 last = first + blockDim.x < a.f.nblocks ? first + blockDim.x : a.f.nblocks;
-  const u64 b0 = a.start + a.offsets[first], b1 = a.start + a.offsets[last];
-  const u64 w0 = b0 >> 6;
-  const u64 sn = b1 >= b0 ? stage_stream(stage, a.stage_words, a.stream, a.stream_len, w0, (b1 >> 6) - w0 + 2) : 0;
-  __syncthreads();
-  const u64 blk = first + tid;
+  const u64 blk = (u64)blockIdx.x * blockDim.x + tid;
   if (blk >= a.f.nblocks) return;
   const u64 o0 = a.offsets[blk], o1 = a.offsets[blk + 1];
   const u64 pos = a.start + o0;
   Reader r;
-  r.init(a.stream, a.stream_len, pos, stage, w0, sn);
+  r.init(a.stream, a.stream_len, pos);
   T b[S::N];
   u32 rb;
   u32 occ = decode_block<T, S::N>(r, b, a.c, ps, &rb);
@@ -375,6 +352,53 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_var
     return;
   }
   check_loads(pos, rb, occ, a.stream_len, a.flags);
+  int len[4];
+  i64 off = block_origin<D>(a.f, blk, len);
+  scatter_block<T, D>(static_cast<T*>(a.data), a.f, off, len, b, a.owner, a.imin, blk);
+}
+
+// Two-kernel decoder for 4^3 blocks.  k_parse reads each block's bits: its
+// head goes to heads[i] and its bit planes to a plane-major scratch (plane k
+// of block i at planes[k * stride + i], so a warp's stores coalesce).  It
+// holds no values and no shared memory, so far more blocks are in flight than
+// in k_decode_*, whose plane store and value registers bound their occupancy.
+// k_finish rebuilds the values and scatters them.
+template <class T, int D, bool VAR>
+__global__ void __launch_bounds__(128, 8) k_parse(DecodeArgs a, SplitArgs sa) {
+  typedef KernelShape<T, D> S;
+  const u64 blk = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (blk >= a.f.nblocks) return;
+  u64 o0 = 0, o1 = 0, pos;
+  if (VAR) {
+    o0 = a.offsets[blk];
+    o1 = a.offsets[blk + 1];
+    pos = a.start + o0;
+  } else {
+    pos = a.start + blk * (u64)a.c.maxbits;
+  }
+  Reader r;
+  r.init(a.stream, a.stream_len, pos);
+  PlaneStore ps{sa.planes + blk, (int)sa.stride};
+  BlockHead h;
+  u32 rb;
+  u32 occ = parse_block<T, S::N>(r, a.c, ps, h, &rb);
+  if (VAR && (o1 < o0 || (u64)occ != o1 - o0)) {
+    atomicOr(a.flags, FLAG_BAD_INDEX);
+    return;
+  }
+  check_loads(pos, rb, occ, a.stream_len, a.flags);
+  sa.heads[blk] = h.pack();
+}
+
+template <class T, int D>
+__global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_finish(DecodeArgs a, SplitArgs sa) {
+  typedef KernelShape<T, D> S;
+  const u64 blk = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (blk >= a.f.nblocks || (*(volatile unsigned*)a.flags & FLAG_BAD_INDEX)) return;
+  PlaneStore ps{sa.planes + blk, (int)sa.stride};
+  const BlockHead h = BlockHead::unpack(sa.heads[blk]);
+  T b[S::N];
+  finish_block<T, S::N>(h, b, ps);
   int len[4];
   i64 off = block_origin<D>(a.f, blk, len);
   scatter_block<T, D>(static_cast<T*>(a.data), a.f, off, len, b, a.owner, a.imin, blk);

@@ -321,7 +321,7 @@ def desc_of(shape, dtype, config: ZfpConfig, strides=None) -> ZfpDesc:
 
 
 KERNEL_KINDS = ["encode_fixed", "encode_var", "scan", "pack", "decode_fixed", "decode_var", "walk", "claim",
-                "offsets"]
+                "offsets", "parse", "finish"]
 
 
 def timing_enable(on: bool = True):
