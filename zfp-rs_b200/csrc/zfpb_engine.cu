@@ -266,36 +266,48 @@ __device__ __forceinline__ u64 slot_bits(const u64* slot, u64 local, u32 take) {
   return take < 64 ? x & ((1ull << take) - 1) : x;
 }
 
+// One warp per 32 consecutive blocks.  The warp's blocks own a contiguous run
+// of stream words; lane l assembles words l, l + 32, ... of that run, finding
+// each word's owner among the warp's block offsets (kept in shared memory), so
+// slot reads and stream writes are coalesced and the lanes' loads do not wait
+// on one another.  A word that runs past its owner's end takes the rest of its
+// bits from the blocks after it.
 __global__ void __launch_bounds__(256) k_pack(PackArgs a) {
-  const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.nblocks) return;
-  const u64 p0 = a.start + a.off[i], p1 = a.start + a.off[i + 1];
-  u64 wlo = (p0 + 63) >> 6;
-  const u64 whi = (p1 + 63) >> 6;
-  if (i == 0) wlo = a.start >> 6;
-  for (u64 w = wlo; w < whi; w++) {
+  __shared__ u64 soff[8][33];
+  const u32 wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const u64 b0 = ((u64)blockIdx.x * 8 + wib) * 32;
+  if (b0 >= a.nblocks) return;
+  const u32 nb = (u32)(a.nblocks - b0 < 32 ? a.nblocks - b0 : 32);
+  u64* po = soff[wib];
+  for (u32 t = lane; t <= nb; t += 32) po[t] = a.start + a.off[b0 + t];
+  __syncwarp();
+  const u64 wbeg = b0 == 0 ? a.start >> 6 : (po[0] + 63) >> 6;
+  const u64 wend = (po[nb] + 63) >> 6;
+  u32 j = 0;
+  for (u64 w = wbeg + lane; w < wend; w += 32) {
     u64 v = 0;
     u32 fill = 0;
     u64 pos = w << 6;
-    if (i == 0 && w == (a.start >> 6)) {
+    if (b0 == 0 && w == (a.start >> 6)) {
       v = a.init_word;
       fill = (u32)(a.start & 63);
       pos = a.start;
     }
-    u64 j = i;
-    u64 pj = p0, qj = p1;
-    while (fill < 64 && j < a.nblocks) {
+    while (j + 1 < nb && po[j + 1] <= pos) j++;  // the block holding bit `pos`
+    u64 blk = b0 + j;
+    u64 pj = po[j], qj = po[j + 1];
+    while (fill < 64 && blk < a.nblocks) {
       u64 local = pos - pj;
       u64 avail = qj - pos;
       u32 take = (u32)(avail < (u64)(64 - fill) ? avail : (u64)(64 - fill));
-      v |= slot_bits(a.slots + j * a.slot_words, local, take) << fill;  // fill < 64
+      v |= slot_bits(a.slots + blk * a.slot_words, local, take) << fill;  // fill < 64
       fill += take;
       pos += take;
       if (pos == qj) {
-        j++;
-        if (j < a.nblocks) {
+        blk++;
+        if (blk < a.nblocks) {
           pj = qj;
-          qj = a.start + a.off[j + 1];
+          qj = a.start + a.off[blk + 1];
         }
       }
     }
