@@ -77,6 +77,34 @@ size_t zfpb_decompress_device(const zfpb_desc* desc, const void* d_stream, size_
 size_t zfpb_compress_device_noalloc(const zfpb_desc* desc, const void* d_field, void* d_stream,
                                     size_t capacity, void* cuda_stream);
 
+/* ---- batches ------------------------------------------------------------
+ *
+ * No counterpart in the reference (zfp-rs codes one field per call).  Many
+ * device-resident arrays of mixed type, dimensionality, size and mode are
+ * coded in a few launches over one flattened list of blocks, instead of one
+ * set of launches (and one synchronisation) per array.  Each array's stream
+ * and decoded values are exactly those of zfpb_compress_device /
+ * zfpb_decompress_device for that array alone.  The first call with a given
+ * item list plans it (tables, scratch, per-class CTA sizes tuned by timing)
+ * and records its launches as a CUDA graph; a later call with the same item
+ * list (same descriptors and buffers) replays the graph.  Up to four plans are
+ * kept per process. */
+typedef struct zfpb_batch_item {
+  zfpb_desc desc;
+  void* d_field;              /* compress: read; decompress: written */
+  void* d_stream;             /* 8-byte aligned; compress: written from bit 0; decompress: read */
+  size_t stream_bytes;        /* compress: capacity; decompress: stream size */
+  uint64_t* d_block_offsets;  /* optional nblocks + 1 block offsets, as for zfpb_compress_device:
+                                 compress writes them, decompress uses them if they match */
+  size_t result;              /* out: stream bytes written / consumed, 0 on failure */
+  int status;                 /* out: 0, or the zfpb_last_error code of this item */
+} zfpb_batch_item;
+
+/* Compress / decompress every item (stream from bit 0, no header).  Returns
+ * the number of items that succeeded; the call returns once all are done. */
+size_t zfpb_compress_batch(zfpb_batch_item* items, size_t n, void* cuda_stream);
+size_t zfpb_decompress_batch(zfpb_batch_item* items, size_t n, void* cuda_stream);
+
 /* Per-kernel timing for profiling: when enabled, every kernel launch of the
  * library is bracketed by CUDA events on its stream.  zfpb_timing_enable
  * clears the totals.  zfpb_timing_read fills, per kernel kind, the summed

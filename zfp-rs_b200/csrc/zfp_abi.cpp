@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 #include <mutex>
 
 #include <cuda_runtime.h>
@@ -1284,6 +1285,59 @@ extern "C" size_t zfpb_decompress_device(const zfpb_desc* d, const void* d_strea
   if (st != zfpb::OK) return fail(st);
   if (cudaStreamSynchronize(s) != cudaSuccess) return fail(zfpb::ERR_CUDA);
   return (size_t)((end + 63) / 64 * 8);
+}
+
+// Batches: every item converted to an engine job, coded together
+// (zfpb::compress_batch / decompress_batch), results written back per item.
+static size_t run_batch_abi(zfpb_batch_item* items, size_t n, void* cuda_stream, bool compress) {
+  if (!items && n) return fail(zfpb::ERR_ARGS);
+  std::vector<zfpb::BatchJob> jobs(n);
+  std::vector<size_t> job_of(n, (size_t)-1);
+  size_t m = 0;
+  for (size_t i = 0; i < n; i++) {
+    zfpb_batch_item& it = items[i];
+    it.result = 0;
+    it.status = zfpb::ERR_ARGS;
+    if (!it.d_field || !it.d_stream || ((uintptr_t)it.d_stream % 8) != 0) continue;
+    Plan p;
+    zfpb::BatchJob& J = jobs[m];
+    if (!call_of_desc(&it.desc, p, J.call, it.d_field)) continue;
+    J.field = it.d_field;
+    J.stream = (u64*)it.d_stream;
+    J.stream_words = it.stream_bytes / 8;
+    J.index = (u64*)it.d_block_offsets;
+    job_of[i] = m++;
+  }
+  cudaStream_t s = (cudaStream_t)cuda_stream;
+  if (m) {
+    zfpb::Status st = compress ? zfpb::compress_batch(jobs.data(), m, s) : zfpb::decompress_batch(jobs.data(), m, s);
+    (void)st;
+  }
+  size_t ok = 0;
+  for (size_t i = 0; i < n; i++) {
+    if (job_of[i] == (size_t)-1) continue;
+    const zfpb::BatchJob& J = jobs[job_of[i]];
+    items[i].status = J.status;
+    if (J.status == zfpb::OK) {
+      items[i].result = (size_t)((J.end_bit + 63) / 64 * 8);
+      ok++;
+    }
+  }
+  g_last_error = 0;
+  for (size_t i = 0; i < n; i++)
+    if (items[i].status != 0) {
+      g_last_error = items[i].status;  // the first failing item's reason
+      break;
+    }
+  return ok;
+}
+
+extern "C" size_t zfpb_compress_batch(zfpb_batch_item* items, size_t n, void* cuda_stream) {
+  return run_batch_abi(items, n, cuda_stream, true);
+}
+
+extern "C" size_t zfpb_decompress_batch(zfpb_batch_item* items, size_t n, void* cuda_stream) {
+  return run_batch_abi(items, n, cuda_stream, false);
 }
 
 // Same stream as zfpb_compress_device, with scratch from the library's static

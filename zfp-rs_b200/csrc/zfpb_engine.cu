@@ -6,6 +6,8 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <memory>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -93,6 +95,7 @@ struct PendingTimer {
 };
 static std::mutex g_timer_mu;
 static bool g_timing = false;
+static thread_local bool g_no_timers = false;  // set while a batch plan is being captured
 static std::vector<PendingTimer> g_pending;
 static double g_ms[K_COUNT];
 static unsigned long long g_count[K_COUNT];
@@ -102,7 +105,7 @@ struct KernelTimer {
   cudaStream_t s;
   cudaEvent_t e0 = nullptr;
   KernelTimer(int k, cudaStream_t st) : kind(k), s(st) {
-    if (g_timing && cudaEventCreate(&e0) == cudaSuccess) cudaEventRecord(e0, s);
+    if (g_timing && !g_no_timers && cudaEventCreate(&e0) == cudaSuccess) cudaEventRecord(e0, s);
   }
   ~KernelTimer() {
     if (!e0) return;
@@ -271,48 +274,55 @@ __device__ __forceinline__ u64 slot_bits(const u64* slot, u64 local, u32 take) {
 // each word's owner among the warp's block offsets (kept in shared memory), so
 // slot reads and stream writes are coalesced and the lanes' loads do not wait
 // on one another.  A word that runs past its owner's end takes the rest of its
-// bits from the blocks after it.
-__global__ void __launch_bounds__(256) k_pack(PackArgs a) {
-  __shared__ u64 soff[8][33];
-  const u32 wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const u64 b0 = ((u64)blockIdx.x * 8 + wib) * 32;
-  if (b0 >= a.nblocks) return;
-  const u32 nb = (u32)(a.nblocks - b0 < 32 ? a.nblocks - b0 : 32);
-  u64* po = soff[wib];
-  for (u32 t = lane; t <= nb; t += 32) po[t] = a.start + a.off[b0 + t];
+// bits from the blocks after it.  Block i's bits start at delta + off[i]; only
+// words below `cap` are written.
+__device__ void pack_warp(const u64* slots, u64 slot_words, const u64* off, u64 delta, u64 nblocks, u64 start,
+                          u64 init_word, u64* out, u64 cap, u64 b0, u64* po, u32 lane) {
+  const u32 nb = (u32)(nblocks - b0 < 32 ? nblocks - b0 : 32);
+  for (u32 t = lane; t <= nb; t += 32) po[t] = delta + off[b0 + t];
   __syncwarp();
-  const u64 wbeg = b0 == 0 ? a.start >> 6 : (po[0] + 63) >> 6;
+  const u64 wbeg = b0 == 0 ? start >> 6 : (po[0] + 63) >> 6;
   const u64 wend = (po[nb] + 63) >> 6;
   u32 j = 0;
   for (u64 w = wbeg + lane; w < wend; w += 32) {
     u64 v = 0;
     u32 fill = 0;
     u64 pos = w << 6;
-    if (b0 == 0 && w == (a.start >> 6)) {
-      v = a.init_word;
-      fill = (u32)(a.start & 63);
-      pos = a.start;
+    if (b0 == 0 && w == (start >> 6)) {
+      v = init_word;
+      fill = (u32)(start & 63);
+      pos = start;
     }
     while (j + 1 < nb && po[j + 1] <= pos) j++;  // the block holding bit `pos`
     u64 blk = b0 + j;
     u64 pj = po[j], qj = po[j + 1];
-    while (fill < 64 && blk < a.nblocks) {
+    while (fill < 64 && blk < nblocks) {
       u64 local = pos - pj;
       u64 avail = qj - pos;
       u32 take = (u32)(avail < (u64)(64 - fill) ? avail : (u64)(64 - fill));
-      v |= slot_bits(a.slots + blk * a.slot_words, local, take) << fill;  // fill < 64
+      v |= slot_bits(slots + blk * slot_words, local, take) << fill;  // fill < 64
       fill += take;
       pos += take;
       if (pos == qj) {
         blk++;
-        if (blk < a.nblocks) {
+        if (blk < nblocks) {
           pj = qj;
-          qj = a.start + a.off[blk + 1];
+          qj = delta + off[blk + 1];
         }
       }
     }
-    a.out[w] = v;
+    if (w < cap) out[w] = v;
   }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(256) k_pack(PackArgs a) {
+  __shared__ u64 soff[8][33];
+  const u32 wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const u64 b0 = ((u64)blockIdx.x * 8 + wib) * 32;
+  if (b0 >= a.nblocks) return;
+  pack_warp(a.slots, a.slot_words, a.off, a.start, a.nblocks, a.start, a.init_word, a.out, ~0ull, b0, soff[wib],
+            lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -370,16 +380,22 @@ template <class Fn> static cudaError_t for_type(int type, Fn fn) {
     }                                 \
   } while (0)
 
-static cudaError_t scan_lengths(Workspace& ws, const u32* d_len, u64 n, u64* d_off, cudaStream_t s) {
+// Exclusive scan of n lengths into off[0..n] (off[n] = total); `part` holds
+// ceil(n / SCAN_TILE) + 1 words.
+static cudaError_t scan_entries(const u32* d_len, u64 n, u64* d_off, u64* part, cudaStream_t s) {
   u64 tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
-  cudaError_t e = ws.partial.ensure((tiles + 1) * sizeof(u64));
-  if (e != cudaSuccess) return e;
-  u64* part = (u64*)ws.partial.p;
   KernelTimer t(K_SCAN, s);
   k_scan_reduce<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(d_len, n, part);
   k_scan_partials<<<1, 1024, 0, s>>>(part, tiles, d_off + n);
   k_scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(d_len, n, part, d_off);
   return cudaGetLastError();
+}
+
+static cudaError_t scan_lengths(Workspace& ws, const u32* d_len, u64 n, u64* d_off, cudaStream_t s) {
+  u64 tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  cudaError_t e = ws.partial.ensure((tiles + 1) * sizeof(u64));
+  if (e != cudaSuccess) return e;
+  return scan_entries(d_len, n, d_off, (u64*)ws.partial.p, s);
 }
 
 // Threads and shared memory for the fixed-size encoder: stage of the CTA's
@@ -618,6 +634,480 @@ Status decompress(const Call& call, const u64* d_in, u64 len, u64 start, void* d
   if (fl & FLAG_BAD_INDEX) return ERR_CUDA;
   return (fl & FLAG_TRUNCATED) ? ERR_TRUNCATED : OK;
 }
+
+// ---------------------------------------------------------------------------
+// Batches (compress_batch / decompress_batch).
+//
+// Planning: jobs are cut into tiles of up to 128 consecutive blocks of one
+// array and grouped by (type, dims); per class one launch codes all its tiles.
+// Scratch (block slots for compress, the plane scratch for 3D decompress) is
+// bounded per round, and rounds run back to back on the stream.  A plan keeps
+// its tables, scratch and a CUDA graph of its launches; a later call with the
+// same jobs replays the graph.  Tuning: the first run of a (pass, type, dims)
+// class times its kernel at 32, 64 and 128 threads per CTA (the tiles are the
+// same, a CTA's threads take its blocks in turn) and keeps the fastest for
+// every later plan.
+// ---------------------------------------------------------------------------
+
+static constexpr u32 BATCH_TILE = 128;
+static constexpr u64 BATCH_ROUND_BYTES = 8ull << 30;  // slot or plane scratch per round
+
+__global__ void __launch_bounds__(256) k_pack_batch(BatchArgs a) {
+  __shared__ u64 soff[8][33];
+  const BatchTile t = a.tiles[blockIdx.x];
+  const u32 wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const u64 b0 = t.first + (u64)wib * 32;
+  if (b0 >= t.first + t.count) return;
+  const BatchItem* it = a.items + t.item;
+  const u64* off = a.offsets + it->len_base;
+  const u64 n = it->f.nblocks;
+  const u64 delta = 0ull - off[0];
+  pack_warp(a.slots + it->slot_base, it->slot_words, off, delta, n, 0, 0, it->stream, it->stream_words, b0,
+            soff[wib], lane);
+  if (it->index) {
+    const u64 e = b0 + 32 < n ? b0 + 32 : n;
+    for (u64 i = b0 + lane; i < e; i += 32) it->index[i] = off[i] + delta;
+    if (e == n && lane == 0) it->index[n] = off[n] + delta;
+  }
+}
+
+// End bit of each item of [first, first + n): compress from the scanned
+// lengths; decompress from i * maxbits, the walker's offsets or the index.
+__global__ void k_batch_ends(BatchArgs a, u32 first, u32 n, int compress, u64* ends) {
+  const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const BatchItem* it = a.items + first + i;
+  const u64 nb = it->f.nblocks;
+  u64 e;
+  if (compress) e = a.offsets[it->len_base + nb] - a.offsets[it->len_base];
+  else if (it->fixed) e = nb * (u64)it->c.maxbits;
+  else if (it->walk) e = a.offsets[it->len_base + nb];
+  else e = it->index[nb];
+  ends[first + i] = e;
+}
+
+namespace {
+
+enum BatchPass { PASS_ENCODE = 0, PASS_DECODE = 1, PASS_PARSE = 2, PASS_FINISH = 3 };
+
+struct BatchLaunch {
+  int pass, type, dims;
+  u32 tile0, ntiles;
+  int threads;  // 0: tune on first run
+};
+
+struct BatchRound {
+  u32 item0, nitems;
+  std::vector<BatchLaunch> launches;
+  u32 ptile0 = 0, nptiles = 0;       // compress: pack tiles
+  u64 entries = 0;                   // lengths / offsets entries
+  std::vector<std::pair<int, std::pair<u32, u32>>> walks;  // (type*8+dims, (first, count) in walk list)
+};
+
+struct BatchPlan {
+  bool compress;
+  int device;
+  std::vector<char> key;
+  std::vector<BatchItem> items;
+  std::vector<u32> job_of_item;
+  std::vector<BatchTile> tiles;
+  std::vector<u32> walk;
+  std::vector<BatchRound> rounds;
+  u64 max_entries = 0, max_slot_words = 0, max_cols = 0, max_walk = 0;
+  Buf d_items, d_tiles, d_walk, slots, lengths, offsets, partial, flags, planes, heads, walk_planes, ends;
+  u64* h_ends = nullptr;
+  unsigned* h_flags = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  bool capture_tried = false;
+  ~BatchPlan() {
+    if (graph) cudaGraphExecDestroy(graph);
+    for (Buf* b : {&d_items, &d_tiles, &d_walk, &slots, &lengths, &offsets, &partial, &flags, &planes, &heads,
+                   &walk_planes, &ends})
+      if (b->p) cudaFree(b->p);
+    if (h_ends) cudaFreeHost(h_ends);
+    if (h_flags) cudaFreeHost(h_flags);
+  }
+};
+
+std::mutex g_batch_mu;
+std::vector<std::unique_ptr<BatchPlan>> g_plans;  // most recently used last
+std::map<int, int> g_tuned;                          // (pass, type, dims) -> threads
+
+int tune_key(int pass, int type, int dims) { return (pass * 8 + type) * 8 + dims; }
+
+std::vector<int> thread_candidates(int pass, int type, int dims) {
+  if (pass == PASS_PARSE || pass == PASS_FINISH) return {128, 64, 32};
+  std::vector<int> c;
+  for (int th : {128, 64, 32})
+    if (plane_bytes(type, dims) * th <= 200 * 1024) c.push_back(th);
+  return c;
+}
+
+cudaError_t launch_pass(const BatchLaunch& L, const BatchArgs& a0, int threads, cudaStream_t s) {
+  BatchArgs a = a0;
+  a.tiles = a0.tiles + L.tile0;
+  return for_type(L.type, [&](auto* tp) {
+    using T = std::remove_pointer_t<decltype(tp)>;
+    switch (L.pass) {
+      case PASS_ENCODE: return Launch<T>::encode_batch(L.dims, a, L.ntiles, threads, s);
+      case PASS_DECODE: return Launch<T>::decode_batch(L.dims, a, L.ntiles, threads, s);
+      case PASS_PARSE: return Launch<T>::parse_batch(a, L.ntiles, threads, s);
+      default: return Launch<T>::finish_batch(a, L.ntiles, threads, s);
+    }
+  });
+}
+
+int kind_of_pass(int pass) {
+  return pass == PASS_ENCODE ? K_ENCODE_VAR : pass == PASS_DECODE ? K_DECODE_VAR : pass == PASS_PARSE ? K_PARSE
+                                                                                                        : K_FINISH;
+}
+
+// Pick the CTA size of a class by timing each candidate on its real tiles
+// (the kernels are idempotent: a rerun writes the same bytes).
+cudaError_t tune_launch(const BatchLaunch& L, const BatchArgs& a, cudaStream_t s, int* best) {
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best_ms = 1e30f;
+  *best = 128;
+  cudaError_t err = cudaSuccess;
+  for (int th : thread_candidates(L.pass, L.type, L.dims)) {
+    err = launch_pass(L, a, th, s);  // warm
+    if (err != cudaSuccess) break;
+    cudaEventRecord(e0, s);
+    err = launch_pass(L, a, th, s);
+    cudaEventRecord(e1, s);
+    if (err != cudaSuccess) break;
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      *best = th;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return err;
+}
+
+// Issue every launch of the plan on s (and, when tune is set, tune the
+// classes not tuned yet), then copy the ends and flags to pinned memory.
+cudaError_t run_plan(BatchPlan& P, cudaStream_t s, bool tune) {
+  BatchArgs a{};
+  a.items = (const BatchItem*)P.d_items.p;
+  a.tiles = (const BatchTile*)P.d_tiles.p;
+  a.slots = (u64*)P.slots.p;
+  a.lengths = (u32*)P.lengths.p;
+  a.offsets = (u64*)P.offsets.p;
+  a.flags = (unsigned*)P.flags.p;
+  a.planes = (u64*)P.planes.p;
+  a.plane_stride = P.max_cols;
+  a.heads = (u64*)P.heads.p;
+  a.walk_planes = (u64*)P.walk_planes.p;
+  const u32 nitems = (u32)P.items.size();
+  cudaError_t e = cudaMemsetAsync(P.flags.p, 0, nitems * sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  for (BatchRound& R : P.rounds) {
+    if (!P.compress) {
+      for (auto& w : R.walks) {
+        BatchArgs aw = a;
+        aw.walk_items = (const u32*)P.d_walk.p + w.second.first;
+        aw.nwalk = w.second.second;
+        KernelTimer t(K_WALK, s);
+        e = for_type(w.first / 8, [&](auto* tp) {
+          using T = std::remove_pointer_t<decltype(tp)>;
+          return Launch<T>::walk_batch(w.first % 8, aw, s);
+        });
+        if (e != cudaSuccess) return e;
+      }
+    }
+    for (BatchLaunch& L : R.launches) {
+      int th = L.threads;
+      if (!th) {
+        auto it = g_tuned.find(tune_key(L.pass, L.type, L.dims));
+        if (it != g_tuned.end()) {
+          th = it->second;
+        } else if (tune) {
+          e = tune_launch(L, a, s, &th);
+          if (e != cudaSuccess) return e;
+          g_tuned[tune_key(L.pass, L.type, L.dims)] = th;
+        } else {
+          th = thread_candidates(L.pass, L.type, L.dims)[0];
+        }
+        L.threads = th;
+      }
+      KernelTimer t(kind_of_pass(L.pass), s);
+      e = launch_pass(L, a, th, s);
+      if (e != cudaSuccess) return e;
+    }
+    if (P.compress) {
+      e = scan_entries(a.lengths, R.entries, a.offsets, (u64*)P.partial.p, s);
+      if (e != cudaSuccess) return e;
+      BatchArgs ap = a;
+      ap.tiles = a.tiles + R.ptile0;
+      {
+        KernelTimer t(K_PACK, s);
+        k_pack_batch<<<R.nptiles, 256, 0, s>>>(ap);
+      }
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    k_batch_ends<<<(R.nitems + 127) / 128, 128, 0, s>>>(a, R.item0, R.nitems, P.compress ? 1 : 0, (u64*)P.ends.p);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  e = cudaMemcpyAsync(P.h_ends, P.ends.p, nitems * sizeof(u64), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyAsync(P.h_flags, P.flags.p, nitems * sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+}
+
+void append_tiles(BatchPlan& P, u32 item, u64 nblocks, u32 size) {
+  for (u64 b = 0; b < nblocks; b += size) P.tiles.push_back({item, (u32)std::min<u64>(size, nblocks - b), b});
+}
+
+std::vector<char> plan_key(const BatchJob* jobs, size_t n, bool compress, int dev) {
+  std::vector<char> k(sizeof(int) * 2 + n * sizeof(BatchJob));
+  int hdr[2] = {compress ? 1 : 0, dev};
+  memcpy(k.data(), hdr, sizeof(hdr));
+  for (size_t i = 0; i < n; i++) {
+    BatchJob j = jobs[i];
+    j.end_bit = 0;
+    j.status = OK;
+    memcpy(k.data() + sizeof(hdr) + i * sizeof(BatchJob), &j, sizeof(BatchJob));
+  }
+  return k;
+}
+
+// Build a plan for the jobs that go through the batch kernels (batched[]).
+cudaError_t build_plan(BatchPlan& P, const BatchJob* jobs, const std::vector<u32>& batched) {
+  // Order items by round; within a round, by class, so a class's tiles are contiguous.
+  std::vector<std::vector<u32>> rounds;
+  {
+    std::vector<u32> cur;
+    u64 bytes = 0;
+    for (u32 j : batched) {
+      const Call& c = jobs[j].call;
+      u64 need;
+      if (P.compress) {
+        need = c.f.nblocks * ((block_bits(c.c, c.type, c.dims) + 63) / 64 + 1) * sizeof(u64);
+      } else {
+        need = c.dims == 3 ? c.f.nblocks * 64 * sizeof(u64) : 0;
+      }
+      if (!cur.empty() && bytes + need > BATCH_ROUND_BYTES) {
+        rounds.push_back(cur);
+        cur.clear();
+        bytes = 0;
+      }
+      cur.push_back(j);
+      bytes += need;
+    }
+    if (!cur.empty()) rounds.push_back(cur);
+  }
+  for (auto& rj : rounds) {
+    BatchRound R;
+    R.item0 = (u32)P.items.size();
+    std::stable_sort(rj.begin(), rj.end(), [&](u32 x, u32 y) {
+      return jobs[x].call.type * 8 + jobs[x].call.dims < jobs[y].call.type * 8 + jobs[y].call.dims;
+    });
+    u64 slot = 0, entries = 0, cols = 0;
+    for (u32 j : rj) {
+      const BatchJob& J = jobs[j];
+      BatchItem it{};
+      it.f = J.call.f;
+      it.c = J.call.c;
+      it.data = J.field;
+      it.stream = J.stream;
+      it.stream_words = J.stream_words;
+      it.index = J.index;
+      it.fixed = fixed_size_blocks(J.call) ? 1 : 0;
+      it.len_base = entries;
+      entries += J.call.f.nblocks + 1;
+      if (P.compress) {
+        it.slot_words = (block_bits(J.call.c, J.call.type, J.call.dims) + 63) / 64 + 1;
+        it.slot_base = slot;
+        slot += J.call.f.nblocks * it.slot_words;
+      } else {
+        it.walk = (!it.fixed && !J.index) ? 1 : 0;
+        if (J.call.dims == 3) {
+          it.plane_base = cols;
+          cols += J.call.f.nblocks;
+        }
+      }
+      P.job_of_item.push_back(j);
+      P.items.push_back(it);
+    }
+    R.nitems = (u32)P.items.size() - R.item0;
+    R.entries = entries;
+    P.max_entries = std::max(P.max_entries, entries);
+    P.max_slot_words = std::max(P.max_slot_words, slot);
+    P.max_cols = std::max(P.max_cols, (cols + 31) & ~31ull);
+    // Launches per class.
+    u32 i = R.item0;
+    while (i < R.item0 + R.nitems) {
+      const int type = jobs[P.job_of_item[i]].call.type, dims = jobs[P.job_of_item[i]].call.dims;
+      u32 e = i;
+      while (e < R.item0 + R.nitems && jobs[P.job_of_item[e]].call.type == type &&
+             jobs[P.job_of_item[e]].call.dims == dims)
+        e++;
+      u32 t0 = (u32)P.tiles.size();
+      for (u32 k = i; k < e; k++) append_tiles(P, k, P.items[k].f.nblocks, BATCH_TILE);
+      u32 nt = (u32)P.tiles.size() - t0;
+      if (P.compress) {
+        R.launches.push_back({PASS_ENCODE, type, dims, t0, nt, 0});
+      } else if (dims == 3) {
+        R.launches.push_back({PASS_PARSE, type, dims, t0, nt, 0});
+        R.launches.push_back({PASS_FINISH, type, dims, t0, nt, 0});
+      } else {
+        R.launches.push_back({PASS_DECODE, type, dims, t0, nt, 0});
+      }
+      if (!P.compress) {
+        u32 w0 = (u32)P.walk.size();
+        for (u32 k = i; k < e; k++)
+          if (P.items[k].walk) P.walk.push_back(k);
+        u32 nw = (u32)P.walk.size() - w0;
+        if (nw) {
+          R.walks.push_back({type * 8 + dims, {w0, nw}});
+          P.max_walk = std::max<u64>(P.max_walk, nw);
+        }
+      }
+      i = e;
+    }
+    if (P.compress) {
+      R.ptile0 = (u32)P.tiles.size();
+      for (u32 k = R.item0; k < R.item0 + R.nitems; k++) append_tiles(P, k, P.items[k].f.nblocks, 256);
+      R.nptiles = (u32)P.tiles.size() - R.ptile0;
+    }
+    P.rounds.push_back(std::move(R));
+  }
+  const u64 nitems = P.items.size();
+  cudaError_t e;
+  if ((e = P.d_items.ensure(nitems * sizeof(BatchItem))) != cudaSuccess) return e;
+  if ((e = P.d_tiles.ensure(std::max<size_t>(1, P.tiles.size()) * sizeof(BatchTile))) != cudaSuccess) return e;
+  if ((e = P.flags.ensure(nitems * sizeof(unsigned))) != cudaSuccess) return e;
+  if ((e = P.ends.ensure(nitems * sizeof(u64))) != cudaSuccess) return e;
+  if ((e = P.offsets.ensure((P.max_entries + 1) * sizeof(u64))) != cudaSuccess) return e;
+  if (P.compress) {
+    if ((e = P.slots.ensure((P.max_slot_words + 1) * sizeof(u64))) != cudaSuccess) return e;
+    if ((e = P.lengths.ensure((P.max_entries + 1) * sizeof(u32))) != cudaSuccess) return e;
+    if ((e = P.partial.ensure(((P.max_entries + SCAN_TILE - 1) / SCAN_TILE + 1) * sizeof(u64))) != cudaSuccess)
+      return e;
+  } else {
+    if (P.max_cols) {
+      if ((e = P.planes.ensure(64 * P.max_cols * sizeof(u64))) != cudaSuccess) return e;
+      if ((e = P.heads.ensure(P.max_cols * sizeof(u64))) != cudaSuccess) return e;
+    }
+    if (!P.walk.empty()) {
+      if ((e = P.d_walk.ensure(P.walk.size() * sizeof(u32))) != cudaSuccess) return e;
+      if ((e = P.walk_planes.ensure(256 * P.max_walk * sizeof(u64))) != cudaSuccess) return e;
+    }
+  }
+  if ((e = cudaMallocHost((void**)&P.h_ends, nitems * sizeof(u64))) != cudaSuccess) return e;
+  if ((e = cudaMallocHost((void**)&P.h_flags, nitems * sizeof(unsigned))) != cudaSuccess) return e;
+  if ((e = cudaMemcpy(P.d_items.p, P.items.data(), nitems * sizeof(BatchItem), cudaMemcpyHostToDevice)) !=
+      cudaSuccess)
+    return e;
+  if (!P.tiles.empty() && (e = cudaMemcpy(P.d_tiles.p, P.tiles.data(), P.tiles.size() * sizeof(BatchTile),
+                                          cudaMemcpyHostToDevice)) != cudaSuccess)
+    return e;
+  if (!P.walk.empty() &&
+      (e = cudaMemcpy(P.d_walk.p, P.walk.data(), P.walk.size() * sizeof(u32), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return e;
+  return cudaSuccess;
+}
+
+// Run the jobs that the batch kernels can take, through a cached plan.
+Status run_batch(BatchJob* jobs, size_t n, bool compress, cudaStream_t s) {
+  std::vector<u32> batched, single;
+  for (size_t i = 0; i < n; i++) {
+    BatchJob& J = jobs[i];
+    J.status = OK;
+    J.end_bit = 0;
+    const Call& c = J.call;
+    if (c.f.nblocks == 0) continue;
+    if (!compress && strides_may_alias(c.f, c.dims)) single.push_back((u32)i);
+    else batched.push_back((u32)i);
+  }
+  if (!batched.empty()) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(g_batch_mu);
+    std::vector<char> key = plan_key(jobs, n, compress, dev);
+    BatchPlan* P = nullptr;
+    for (size_t i = 0; i < g_plans.size(); i++)
+      if (g_plans[i]->key == key) {
+        std::unique_ptr<BatchPlan> keep = std::move(g_plans[i]);
+        g_plans.erase(g_plans.begin() + i);
+        g_plans.push_back(std::move(keep));
+        P = g_plans.back().get();
+        break;
+      }
+    if (P && P->graph) {
+      if (cudaGraphLaunch(P->graph, s) != cudaSuccess) return ERR_CUDA;
+    } else if (P && P->capture_tried) {
+      if (run_plan(*P, s, true) != cudaSuccess) return ERR_CUDA;
+    } else {
+      if (!P) {
+        while (g_plans.size() >= 4) g_plans.erase(g_plans.begin());
+        auto np = std::make_unique<BatchPlan>();
+        np->compress = compress;
+        np->device = dev;
+        np->key = key;
+        if (build_plan(*np, jobs, batched) != cudaSuccess) {
+          cudaGetLastError();
+          return ERR_CUDA;
+        }
+        g_plans.push_back(std::move(np));
+        P = g_plans.back().get();
+      }
+      if (run_plan(*P, s, true) != cudaSuccess) return ERR_CUDA;
+      if (cudaStreamSynchronize(s) != cudaSuccess) return ERR_CUDA;
+      // Capture the launches for the next call with the same jobs (once: a
+      // stream that cannot be captured, like the legacy default stream, runs
+      // the launches directly every time).
+      cudaGraph_t g = nullptr;
+      P->capture_tried = true;
+      g_no_timers = true;
+      bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (ok) {
+        cudaError_t re = run_plan(*P, s, false);
+        ok = cudaStreamEndCapture(s, &g) == cudaSuccess && re == cudaSuccess && g;
+      }
+      g_no_timers = false;
+      if (ok && cudaGraphInstantiate(&P->graph, g, 0) != cudaSuccess) P->graph = nullptr;
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) return ERR_CUDA;
+    for (size_t k = 0; k < P->items.size(); k++) {
+      BatchJob& J = jobs[P->job_of_item[k]];
+      J.end_bit = P->h_ends[k];
+      const unsigned fl = P->h_flags[k];
+      if (compress) {
+        if ((J.end_bit + 63) / 64 > J.stream_words) J.status = ERR_OVERFLOW;
+      } else if (fl & FLAG_BAD_INDEX) {
+        single.push_back(P->job_of_item[k]);  // index does not match: walk this one alone
+      } else if (fl & FLAG_TRUNCATED) {
+        J.status = ERR_TRUNCATED;
+      }
+    }
+  }
+  for (u32 i : single) {
+    BatchJob& J = jobs[i];
+    u64 end = 0;
+    Status st = compress ? ERR_ARGS
+                         : decompress(J.call, J.stream, J.stream_words, 0, J.field, &end, nullptr, s);
+    J.status = st;
+    J.end_bit = end;
+  }
+  Status all = OK;
+  for (size_t i = 0; i < n; i++)
+    if (jobs[i].status != OK) all = jobs[i].status;
+  return all;
+}
+
+}  // namespace
+
+Status compress_batch(BatchJob* jobs, size_t n, cudaStream_t s) { return run_batch(jobs, n, true, s); }
+Status decompress_batch(BatchJob* jobs, size_t n, cudaStream_t s) { return run_batch(jobs, n, false, s); }
 
 }  // namespace zfpb
 

@@ -113,6 +113,69 @@ Status compress(const Call& call, const void* d_field, u64* d_out, u64 cap, u64 
 Status decompress(const Call& call, const u64* d_in, u64 len, u64 start, void* d_field, u64* end_bit,
                   const u64* d_offsets, cudaStream_t s);
 
+// ---- batches ---------------------------------------------------------------
+//
+// A batch codes many arrays of mixed type, dimensionality, size and mode in a
+// few launches over a flattened block work list.  Work is cut into tiles
+// (up to one CTA's worth of consecutive blocks of one array); the arrays of one
+// (type, dims) class share one launch per kernel.
+
+// Device-side descriptor of one array of a batch.
+struct BatchItem {
+  FieldGeom f;
+  CodecParams c;
+  void* data;        // the field (compress: read, decompress: written)
+  u64* stream;       // compress: written from bit 0; decompress: read from bit 0
+  u64 stream_words;  // compress: capacity; decompress: stream length
+  u64* index;        // optional block offsets (nblocks + 1): compress writes, decompress tries
+  u64 slot_base;     // compress: first word of this array's block slots
+  u64 slot_words;    // compress: words per block slot
+  u64 len_base;      // this array's nblocks + 1 entries in the batch lengths / offsets
+  u64 plane_base;    // 3D decompress: column of block 0 in the plane scratch
+  u32 fixed;         // every block takes exactly maxbits bits
+  u32 walk;          // decompress: offsets come from the batch walker
+};
+
+// Blocks [first, first + count) of items[item].
+struct BatchTile {
+  u32 item;
+  u32 count;
+  u64 first;
+};
+
+struct BatchArgs {
+  const BatchItem* items;
+  const BatchTile* tiles;  // this launch's tiles, one per CTA
+  u64* slots;
+  u32* lengths;
+  u64* offsets;
+  unsigned* flags;         // per item: FLAG_TRUNCATED, FLAG_BAD_INDEX
+  u64* planes;             // 3D decompress plane scratch, plane k of column j at planes[k * plane_stride + j]
+  u64 plane_stride;
+  u64* heads;
+  const u32* walk_items;   // items whose offsets the walker finds
+  u32 nwalk;
+  u64* walk_planes;        // one plane store per walking thread
+};
+
+// One array of a batch call (host side).
+struct BatchJob {
+  Call call;
+  void* field;
+  u64* stream;
+  u64 stream_words;
+  u64* index;
+  u64 end_bit;    // out: stream bits written / read
+  Status status;  // out
+};
+
+// Compress / decompress every job; each job's status and end_bit are set.
+// Returns OK when every job succeeded.  Plans (tables, scratch and a CUDA
+// graph of the launches) are cached by the jobs' contents, so calling again
+// with the same jobs replays the graph.
+Status compress_batch(BatchJob* jobs, size_t n, cudaStream_t s);
+Status decompress_batch(BatchJob* jobs, size_t n, cudaStream_t s);
+
 // Kernel launchers, one instantiation per scalar type (zfpb_inst_*.cu).
 template <class T> struct Launch {
   static cudaError_t encode_fixed(const Call& call, const EncodeFixedArgs& a, u64 ctas, int threads,
@@ -121,6 +184,12 @@ template <class T> struct Launch {
   static cudaError_t decode_fixed(const Call& call, const DecodeArgs& a, cudaStream_t s);
   static cudaError_t decode_var(const Call& call, const DecodeArgs& a, cudaStream_t s);
   static cudaError_t walk(const Call& call, const DecodeArgs& a, cudaStream_t s);
+  // Batches: one launch over `ntiles` tiles of (T, dims) arrays.
+  static cudaError_t encode_batch(int dims, const BatchArgs& a, u32 ntiles, int threads, cudaStream_t s);
+  static cudaError_t decode_batch(int dims, const BatchArgs& a, u32 ntiles, int threads, cudaStream_t s);
+  static cudaError_t parse_batch(const BatchArgs& a, u32 ntiles, int threads, cudaStream_t s);
+  static cudaError_t finish_batch(const BatchArgs& a, u32 ntiles, int threads, cudaStream_t s);
+  static cudaError_t walk_batch(int dims, const BatchArgs& a, cudaStream_t s);
   // Two-kernel decoder, 3D fields only.
   static cudaError_t parse(const Call& call, const DecodeArgs& a, const SplitArgs& sa, bool var, cudaStream_t s);
   static cudaError_t finish(const Call& call, const DecodeArgs& a, const SplitArgs& sa, cudaStream_t s);

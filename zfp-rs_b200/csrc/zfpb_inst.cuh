@@ -96,6 +96,62 @@ cudaError_t Launch<T>::finish(const Call& call, const DecodeArgs& a, const Split
   k_finish<T, 3><<<grid_of(a.f.nblocks, 128), 128, 0, s>>>(a, sa);
   return cudaGetLastError();
 }
+template <class T, int D>
+static cudaError_t encode_batch_d(const BatchArgs& a, u32 ntiles, int th, cudaStream_t s) {
+  size_t smem = plane_smem<T, D>(th);
+  cudaError_t e = set_smem<T, D>((const void*)k_encode_batch<T, D>, smem);
+  if (e != cudaSuccess) return e;
+  k_encode_batch<T, D><<<ntiles, th, smem, s>>>(a);
+  return cudaGetLastError();
+}
+template <class T, int D>
+static cudaError_t decode_batch_d(const BatchArgs& a, u32 ntiles, int th, cudaStream_t s) {
+  size_t smem = plane_smem<T, D>(th);
+  cudaError_t e = set_smem<T, D>((const void*)k_decode_batch<T, D>, smem);
+  if (e != cudaSuccess) return e;
+  k_decode_batch<T, D><<<ntiles, th, smem, s>>>(a);
+  return cudaGetLastError();
+}
+template <class T, int D> static cudaError_t walk_batch_d(const BatchArgs& a, cudaStream_t s) {
+  k_walk_batch<T, D><<<(a.nwalk + 63) / 64, 64, 0, s>>>(a);
+  return cudaGetLastError();
+}
+template <class T>
+cudaError_t Launch<T>::encode_batch(int dims, const BatchArgs& a, u32 ntiles, int threads, cudaStream_t s) {
+  switch (dims) {
+    case 1: return encode_batch_d<T, 1>(a, ntiles, threads, s);
+    case 2: return encode_batch_d<T, 2>(a, ntiles, threads, s);
+    case 3: return encode_batch_d<T, 3>(a, ntiles, threads, s);
+    default: return encode_batch_d<T, 4>(a, ntiles, threads, s);
+  }
+}
+template <class T>
+cudaError_t Launch<T>::decode_batch(int dims, const BatchArgs& a, u32 ntiles, int threads, cudaStream_t s) {
+  switch (dims) {
+    case 1: return decode_batch_d<T, 1>(a, ntiles, threads, s);
+    case 2: return decode_batch_d<T, 2>(a, ntiles, threads, s);
+    case 3: return decode_batch_d<T, 3>(a, ntiles, threads, s);
+    default: return decode_batch_d<T, 4>(a, ntiles, threads, s);
+  }
+}
+template <class T>
+cudaError_t Launch<T>::parse_batch(const BatchArgs& a, u32 ntiles, int threads, cudaStream_t s) {
+  k_parse_batch<T><<<ntiles, threads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+template <class T>
+cudaError_t Launch<T>::finish_batch(const BatchArgs& a, u32 ntiles, int threads, cudaStream_t s) {
+  k_finish_batch<T><<<ntiles, threads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+template <class T> cudaError_t Launch<T>::walk_batch(int dims, const BatchArgs& a, cudaStream_t s) {
+  switch (dims) {
+    case 1: return walk_batch_d<T, 1>(a, s);
+    case 2: return walk_batch_d<T, 2>(a, s);
+    case 3: return walk_batch_d<T, 3>(a, s);
+    default: return walk_batch_d<T, 4>(a, s);
+  }
+}
 template <class T> cudaError_t Launch<T>::walk(const Call& call, const DecodeArgs& a, cudaStream_t s) {
   ZFPB_DISPATCH(call, walk_d, a, s)
 }

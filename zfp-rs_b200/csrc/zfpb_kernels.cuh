@@ -418,12 +418,161 @@ __global__ void __launch_bounds__(32) k_walk(DecodeArgs a) {
     a.offsets[blk] = rel;
     Reader r;
     r.init(a.stream, a.stream_len, a.start + rel);
-    T b[S::N];
+    BlockHead h;
     u32 rb;
-    u32 occ = decode_block<T, S::N>(r, b, a.c, ps, &rb);
-    rel += occ;
+    rel += parse_block<T, S::N>(r, a.c, ps, h, &rb);
   }
   a.offsets[a.f.nblocks] = rel;
+}
+
+// ---------------------------------------------------------------------------
+// Batches: one CTA per tile (up to 128 consecutive blocks of one array, which
+// the CTA's threads take in turn), the arrays of one (type, dims) class in one
+// launch.  The per-block work is that of the
+// single-array kernels above, with the array's geometry, codec parameters and
+// buffers read from its BatchItem.
+// ---------------------------------------------------------------------------
+
+template <class T, int D>
+__global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_encode_batch(BatchArgs a) {
+  typedef KernelShape<T, D> S;
+  extern __shared__ u64 smem[];
+  const BatchTile t = a.tiles[blockIdx.x];
+  const int tid = threadIdx.x;
+  const BatchItem* it = a.items + t.item;
+  PlaneStore ps{smem + tid, (int)blockDim.x};
+  const CodecParams c = it->c;
+  const u64 sw = it->slot_words;
+  u32* lens = a.lengths + it->len_base;
+  for (u32 j = tid; j < t.count; j += blockDim.x) {
+    const u64 blk = t.first + j;
+    int len[4];
+    i64 off = block_origin<D>(it->f, blk, len);
+    T b[S::N];
+    gather_block<T, D>(static_cast<const T*>(it->data), it->f, off, len, b);
+    Writer<false> w;
+    w.init(a.slots + it->slot_base + blk * sw, 0, sw);
+    u32 bits = encode_block<T, S::N>(w, b, c, ps);
+    w.finish();
+    lens[blk] = bits;
+    if (blk + 1 == it->f.nblocks) lens[blk + 1] = 0;
+  }
+}
+
+// Where block `blk` of an item starts, and where the next one starts (from the
+// item's index, the walker's offsets, or i * maxbits).
+ZFPB_DEV const u64* batch_offsets(const BatchArgs& a, const BatchItem* it) {
+  return it->walk ? a.offsets + it->len_base : it->index;
+}
+
+template <class T, int D>
+__global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_batch(BatchArgs a) {
+  typedef KernelShape<T, D> S;
+  extern __shared__ u64 smem[];
+  const BatchTile t = a.tiles[blockIdx.x];
+  const int tid = threadIdx.x;
+  const BatchItem* it = a.items + t.item;
+  PlaneStore ps{smem + tid, (int)blockDim.x};
+  const CodecParams c = it->c;
+  const u64* offs = batch_offsets(a, it);
+  for (u32 j = tid; j < t.count; j += blockDim.x) {
+    const u64 blk = t.first + j;
+    u64 o0, o1;
+    if (it->fixed) {
+      o0 = blk * (u64)c.maxbits;
+      o1 = o0 + c.maxbits;
+    } else {
+      o0 = offs[blk];
+      o1 = offs[blk + 1];
+    }
+    Reader r;
+    r.init(it->stream, it->stream_words, o0);
+    T b[S::N];
+    u32 rb;
+    u32 occ = decode_block<T, S::N>(r, b, c, ps, &rb);
+    if (o1 < o0 || (u64)occ != o1 - o0) {
+      atomicOr(a.flags + t.item, FLAG_BAD_INDEX);
+      continue;
+    }
+    check_loads(o0, rb, occ, it->stream_words, a.flags + t.item);
+    int len[4];
+    i64 off = block_origin<D>(it->f, blk, len);
+    scatter_block<T, D>(static_cast<T*>(it->data), it->f, off, len, b, nullptr, 0, blk);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(128, 8) k_parse_batch(BatchArgs a) {
+  const BatchTile t = a.tiles[blockIdx.x];
+  const BatchItem* it = a.items + t.item;
+  const CodecParams c = it->c;
+  const u64* offs = batch_offsets(a, it);
+  for (u32 j = threadIdx.x; j < t.count; j += blockDim.x) {
+    const u64 blk = t.first + j;
+    u64 o0, o1;
+    if (it->fixed) {
+      o0 = blk * (u64)c.maxbits;
+      o1 = o0 + c.maxbits;
+    } else {
+      o0 = offs[blk];
+      o1 = offs[blk + 1];
+    }
+    Reader r;
+    r.init(it->stream, it->stream_words, o0);
+    const u64 col = it->plane_base + blk;
+    PlaneStore ps{a.planes + col, (int)a.plane_stride};
+    BlockHead h;
+    u32 rb;
+    u32 occ = parse_block<T, 64>(r, c, ps, h, &rb);
+    if (o1 < o0 || (u64)occ != o1 - o0) {
+      atomicOr(a.flags + t.item, FLAG_BAD_INDEX);
+      continue;
+    }
+    check_loads(o0, rb, occ, it->stream_words, a.flags + t.item);
+    a.heads[col] = h.pack();
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(128, KernelShape<T, 3>::MIN_CTAS) k_finish_batch(BatchArgs a) {
+  const BatchTile t = a.tiles[blockIdx.x];
+  if (*(volatile unsigned*)(a.flags + t.item) & FLAG_BAD_INDEX) return;
+  const BatchItem* it = a.items + t.item;
+  for (u32 j = threadIdx.x; j < t.count; j += blockDim.x) {
+    const u64 blk = t.first + j;
+    const u64 col = it->plane_base + blk;
+    PlaneStore ps{a.planes + col, (int)a.plane_stride};
+    const BlockHead h = BlockHead::unpack(a.heads[col]);
+    T b[64];
+    finish_block<T, 64>(h, b, ps);
+    int len[4];
+    i64 off = block_origin<3>(it->f, blk, len);
+    scatter_block<T, 3>(static_cast<T*>(it->data), it->f, off, len, b, nullptr, 0, blk);
+  }
+}
+
+// Offsets of the items listed in walk_items: one thread per item walks its
+// stream block by block (the stream half of the decode only).
+template <class T, int D>
+__global__ void __launch_bounds__(64) k_walk_batch(BatchArgs a) {
+  typedef KernelShape<T, D> S;
+  const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nwalk) return;
+  const BatchItem* it = a.items + a.walk_items[i];
+  PlaneStore ps{a.walk_planes + i, (int)a.nwalk};
+  const CodecParams c = it->c;
+  u64* off = a.offsets + it->len_base;
+  u64 rel = 0;
+  const u64 n = it->f.nblocks;
+  for (u64 blk = 0; blk < n; blk++) {
+    off[blk] = rel;
+    Reader r;
+    r.init(it->stream, it->stream_words, rel);
+    BlockHead h;
+    u32 rb;
+    rel += parse_block<T, S::N>(r, c, ps, h, &rb);
+  }
+  off[n] = rel;
 }
 
 // Owner map for fields whose strides may alias: every element records the

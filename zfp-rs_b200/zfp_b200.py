@@ -74,6 +74,13 @@ class ZfpDesc(C.Structure):
                 ("minexp", C.c_int32), ("rounding", C.c_int), ("tight_error", C.c_int32)]
 
 
+class ZfpBatchItem(C.Structure):
+    """zfpb_batch_item (include/zfp_b200.h)."""
+
+    _fields_ = [("desc", ZfpDesc), ("d_field", C.c_void_p), ("d_stream", C.c_void_p), ("stream_bytes", C.c_size_t),
+                ("d_block_offsets", C.c_void_p), ("result", C.c_size_t), ("status", C.c_int)]
+
+
 # (name, restype, argtypes) of every function include/zfp.h and include/zfp_b200.h declare.
 _vp, _sz, _u, _u64, _i32, _b = C.c_void_p, C.c_size_t, C.c_uint, C.c_uint64, C.c_int32, C.c_int32
 _F = C.POINTER(ZfpField)
@@ -131,6 +138,8 @@ SIGNATURES = [
     ("zfpb_compress_device", _sz, [C.POINTER(ZfpDesc), _vp, _vp, _sz, _vp, _vp]),
     ("zfpb_decompress_device", _sz, [C.POINTER(ZfpDesc), _vp, _sz, _vp, _vp, _vp]),
     ("zfpb_compress_device_noalloc", _sz, [C.POINTER(ZfpDesc), _vp, _vp, _sz, _vp]),
+    ("zfpb_compress_batch", _sz, [C.POINTER(ZfpBatchItem), _sz, _vp]),
+    ("zfpb_decompress_batch", _sz, [C.POINTER(ZfpBatchItem), _sz, _vp]),
 ]
 DATA_SYMBOLS = ["stream_word_bits", "zfp_codec_version", "zfp_library_version"]
 
@@ -372,3 +381,46 @@ def decompress_device(stream_t, nbytes: int, out, config: ZfpConfig, offsets=Non
     if n == 0:
         raise ZfpError("decompress_device", lib().zfpb_last_error())
     return n
+
+
+def batch_items(fields, configs, streams, nbytes=None, offsets=None):
+    """A ctypes array of zfpb_batch_item for torch CUDA tensors.
+
+    fields[i] is a contiguous CUDA tensor (the input of a compress, the output
+    of a decompress), streams[i] a CUDA tensor holding its stream, nbytes[i]
+    the stream size for a decompress (default: the stream tensor's size), and
+    offsets[i] an optional int64 CUDA tensor of nblocks + 1 block offsets.
+    """
+    n = len(fields)
+    items = (ZfpBatchItem * n)()
+    for i in range(n):
+        f, st = fields[i], streams[i]
+        items[i].desc = desc_of(f.shape, _np_dtype(f.dtype), configs[i])
+        items[i].d_field = f.data_ptr()
+        items[i].d_stream = st.data_ptr()
+        items[i].stream_bytes = nbytes[i] if nbytes is not None else st.numel() * st.element_size()
+        o = offsets[i] if offsets is not None else None
+        items[i].d_block_offsets = o.data_ptr() if o is not None else None
+    return items
+
+
+def compress_batch(items, stream=None):
+    """zfpb_compress_batch over `items` (from batch_items); returns each item's stream bytes."""
+    import torch
+
+    cs = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    ok = lib().zfpb_compress_batch(items, len(items), cs)
+    if ok != len(items):
+        raise ZfpError("compress_batch", lib().zfpb_last_error())
+    return [it.result for it in items]
+
+
+def decompress_batch(items, stream=None):
+    """zfpb_decompress_batch over `items`; returns the bytes each item consumed."""
+    import torch
+
+    cs = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    ok = lib().zfpb_decompress_batch(items, len(items), cs)
+    if ok != len(items):
+        raise ZfpError("decompress_batch", lib().zfpb_last_error())
+    return [it.result for it in items]
