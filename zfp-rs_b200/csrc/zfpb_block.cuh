@@ -746,13 +746,14 @@ __device__ const unsigned short kOnesDoubled[256] = {
     0x0ff0, 0x1fe3, 0x1fe6, 0x3fcf, 0x1fec, 0x3fdb, 0x3fde, 0x7fbf, 0x1ff8, 0x3ff3, 0x3ff6, 0x7fef,
     0x3ffc, 0x7ffb, 0x7ffe, 0xffff};
 
-// The bits of y with every one-bit doubled, as a 128-bit value (lo, hi).
-ZFPB_DEV void double_ones(u64 y, u64& lo, u64& hi) {
+// The bits of y (at most N of them) with every one-bit doubled, as a
+// 128-bit value (lo, hi).
+template <int N> ZFPB_DEV void double_ones(u64 y, u64& lo, u64& hi) {
   lo = 0;
   hi = 0;
   u32 r = 0;  // one-bits below the current byte
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
+  for (int i = 0; i < (N + 7) / 8; i++) {
     const u32 b = (u32)(y >> (8 * i)) & 0xffu;
     const u64 t = __ldg(kOnesDoubled + b);
     const u32 sh = 8 * i + r;  // at most 112
@@ -765,6 +766,89 @@ ZFPB_DEV void double_ones(u64 y, u64& lo, u64& hi) {
     r += __popc(b);
   }
 }
+
+// Plane codes of 1D blocks (4 coefficients) as tables, built at compile time
+// from the same rules as the loops below (bitplane.rs:509-620, 675-790).
+//   kPlane4Enc[n * 16 + x]: the code of plane x with n < 4 significant
+//     coefficients: bits 0-7 the code (verbatim n bits, then the group tests),
+//     bits 8-11 its length, bits 12-14 the new n.
+//   kPlane4Dec[n * 256 + b]: reading a plane from the 8 stream bits b with
+//     n < 4: bits 0-3 the plane, bits 4-7 the code length (0 when the code
+//     does not end within 8 bits), bits 8-10 the new n.
+struct Plane4Tables {
+  unsigned short enc[64];
+  unsigned short dec[1024];
+  constexpr Plane4Tables() : enc(), dec() {
+    for (unsigned n = 0; n < 4; n++) {
+      for (unsigned x = 0; x < 16; x++) {
+        unsigned code = x & ((1u << n) - 1), len = n, nn = n;
+        const unsigned y = x >> n;
+        if (y == 0) {
+          len += 1;  // "0"
+        } else {
+          code |= 1u << len;  // "1": a one follows
+          len += 1;
+          unsigned c = n;
+          while (c < 4) {
+            if (c == 3) {  // the last coefficient's one is implied
+              c = 4;
+              break;
+            }
+            const unsigned b = (x >> c) & 1u;
+            code |= b << len;
+            len += 1;
+            c += 1;
+            if (b) {
+              if ((x >> c) == 0) {  // no more ones: group test "0"
+                len += 1;
+                break;
+              }
+              code |= 1u << len;  // group test "1"
+              len += 1;
+            }
+          }
+          nn = c;
+        }
+        enc[n * 16 + x] = (unsigned short)(code | len << 8 | nn << 12);
+      }
+      for (unsigned b = 0; b < 256; b++) {
+        unsigned pos = n, x = b & ((1u << n) - 1), c = n;
+        bool ok = true;
+        while (c < 4) {
+          if (pos >= 8) {
+            ok = false;
+            break;
+          }
+          const unsigned g = (b >> pos) & 1u;
+          pos += 1;
+          if (!g) break;
+          while (c < 4) {
+            if (c == 3) {
+              x |= 1u << 3;
+              c = 4;
+              break;
+            }
+            if (pos >= 8) {
+              ok = false;
+              break;
+            }
+            const unsigned v = (b >> pos) & 1u;
+            pos += 1;
+            if (v) {
+              x |= 1u << c;
+              c += 1;
+              break;
+            }
+            c += 1;
+          }
+          if (!ok) break;
+        }
+        dec[n * 256 + b] = ok ? (unsigned short)(x | pos << 4 | c << 8) : (unsigned short)0;
+      }
+    }
+  }
+};
+__device__ constexpr Plane4Tables kPlane4{};
 
 // encode_ints (bitplane.rs:509-610) one bit plane at a time.  A plane with
 // n significant coefficients is coded as its low n bits verbatim followed by
@@ -800,8 +884,18 @@ ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore
     bits -= empty;
     u32 k = intprec - empty;
     while (bits != 0 && k > kmin) {
+      if (N <= 16 && n == size) break;  // verbatim tail below
       k--;
       const u64 x = ps.at(k, 0, 1);
+      if constexpr (N == 4) {
+        const u32 e = kPlane4.enc[n * 16 + (u32)x];
+        const u32 len = (e >> 8) & 15u;
+        const u32 take = len < bits ? len : bits;
+        w.put(e & low_mask(take), take);
+        bits -= take;
+        n = e >> 12;
+        continue;
+      }
       if (n == size) {
         const u32 take = size < bits ? size : bits;
         w.put(x & low_mask(take), take);
@@ -815,7 +909,7 @@ ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore
         const u32 hb = 63 - (u32)__clzll((long long)y);
         const u32 c = (u32)__popcll((long long)y);
         u64 elo, ehi;
-        double_ones(y, elo, ehi);
+        double_ones<N>(y, elo, ehi);
         const u32 p = hb + c;  // second copy of the highest one: written as 0
         if (p < 64) elo &= ~(1ull << p);
         else ehi &= ~(1ull << (p - 64));
@@ -838,6 +932,24 @@ ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore
       }
       bits -= take;
       n = nn;
+    }
+    if constexpr (N <= 16) {
+      // Every coefficient significant: the remaining planes go out verbatim,
+      // 64 / size of them per write, cut at the budget.  After the loop above
+      // so that a warp's threads run it together.
+      constexpr u32 per = 64 / size;
+      while (bits != 0 && k > kmin) {
+        u64 chunk = 0;
+        const u32 np = k - kmin < per ? k - kmin : per;
+#pragma unroll
+        for (u32 j = 0; j < per; j++)
+          if (j < np) chunk |= (ps.at(k - 1 - j, 0, 1) & low_mask(size)) << (j * size);
+        const u32 want = np * size;
+        const u32 take = want < bits ? want : bits;
+        w.put(chunk & low_mask(take), take);
+        bits -= take;
+        k -= np;
+      }
     }
     return budget - bits;
   }
@@ -1067,10 +1179,13 @@ ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 in
   r.init(&rd, rd.pos());
   u32 bits = budget, n = 0, m = 0, k = intprec;
   int low = (int)intprec, high = -1;
+  bool done = false;
   while (bits != 0) {
+    if (N <= 16 && n == size) break;  // verbatim tail below
     m = 0;
     if (k <= kmin) {
       k = k - 1;
+      done = true;
       break;
     }
     const u64 lo = r.lo();
@@ -1088,6 +1203,20 @@ ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 in
       }
     }
     k--;
+    if constexpr (N == 4) {
+      const u32 e = kPlane4.dec[n * 256 + (u32)(lo & 0xff)];
+      const u32 len = (e >> 4) & 15u;
+      if (len != 0 && len <= bits) {
+        ps.at(k, 0, 1) = e & 15u;
+        if (high < 0) high = (int)k;
+        low = (int)k;
+        n = e >> 8;
+        m = size;
+        bits -= len;
+        r.advance(len);
+        continue;
+      }
+    }
     u64 x;
     u32 used;
     if (n == size) {
@@ -1182,6 +1311,43 @@ ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 in
     ps.at(k, 0, 1) = x;
     if (high < 0) high = (int)k;
     low = (int)k;
+  }
+  if constexpr (N <= 16) {
+    // Every coefficient significant: verbatim planes, as many at once as the
+    // window's 64 bits hold while more than a plane of budget is left (the
+    // reference reads them one at a time while bits > size, m staying 0),
+    // then a last partial plane.  After the loop above so that a warp's
+    // threads run it together.
+    constexpr u32 per = 64 / size;
+    while (!done && bits != 0) {
+      m = 0;
+      if (k <= kmin) {
+        k = k - 1;
+        break;
+      }
+      const u64 lo = r.lo();
+      k--;
+      if (bits > size) {
+        u32 np = (bits - 1) / size;
+        np = np < per ? np : per;
+        np = np < k + 1 - kmin ? np : k + 1 - kmin;
+#pragma unroll
+        for (u32 j = 0; j < per; j++)
+          if (j < np) ps.at(k - j, 0, 1) = (lo >> (j * size)) & low_mask(size);
+        if (high < 0) high = (int)k;
+        k -= np - 1;
+        low = (int)k;
+        bits -= np * size;
+        r.advance(np * size);
+      } else {
+        ps.at(k, 0, 1) = lo & low_mask(bits);
+        if (high < 0) high = (int)k;
+        low = (int)k;
+        m = bits;
+        r.advance(bits);
+        bits = 0;
+      }
+    }
   }
   if (n == 0) low = (int)intprec;
   rd.init(rd.src, rd.len, r.pos());
