@@ -105,6 +105,41 @@ typedef struct zfpb_batch_item {
 size_t zfpb_compress_batch(zfpb_batch_item* items, size_t n, void* cuda_stream);
 size_t zfpb_decompress_batch(zfpb_batch_item* items, size_t n, void* cuda_stream);
 
+/* ---- serving ------------------------------------------------------------
+ *
+ * No counterpart in the reference.  A serving loop for streams of compress /
+ * decompress requests on device-resident buffers.  Requests are admitted in
+ * arrival order while the device bytes they hold (field, stream and batch
+ * scratch) fit in the budget; admitted requests are coded together in the
+ * next batch as soon as one of `lanes` CUDA streams is free, so requests that
+ * arrive while others run join the next batch and overlap with the batches in
+ * flight.  Each result equals that of the single-array device call.  The
+ * caller keeps the buffers alive until the request is returned by poll. */
+typedef struct zfpb_server zfpb_server;
+
+typedef struct zfpb_request_done {
+  uint64_t tag;       /* as given to zfpb_server_submit */
+  size_t result;      /* stream bytes written / consumed, 0 on failure */
+  int status;         /* 0, or a zfpb_last_error code */
+  double queue_ms;    /* submit -> launch */
+  double latency_ms;  /* submit -> result available */
+} zfpb_request_done;
+
+/* budget_bytes: device memory that admitted requests may hold at once;
+ * lanes: batches in flight at once (0: 2); max_batch: requests per batch
+ * (0: no limit but 4096).  Returns NULL on failure. */
+zfpb_server* zfpb_server_create(size_t budget_bytes, int lanes, size_t max_batch);
+/* Queue one request (decompress = 0: compress item->d_field into
+ * item->d_stream).  Returns 0 if the request is invalid or alone exceeds the
+ * budget. */
+int zfpb_server_submit(zfpb_server* s, const zfpb_batch_item* item, int decompress, uint64_t tag);
+/* Finished requests, up to max, waiting up to wait_ms for the first one. */
+size_t zfpb_server_poll(zfpb_server* s, zfpb_request_done* out, size_t max, int wait_ms);
+/* Submitted requests not yet returned by zfpb_server_poll. */
+size_t zfpb_server_outstanding(zfpb_server* s);
+/* Finish all submitted work, then free the server. */
+void zfpb_server_destroy(zfpb_server* s);
+
 /* Per-kernel timing for profiling: when enabled, every kernel launch of the
  * library is bracketed by CUDA events on its stream.  zfpb_timing_enable
  * clears the totals.  zfpb_timing_read fills, per kernel kind, the summed

@@ -20,6 +20,7 @@
 #include "../../include/zfp.h"
 #include "../../include/zfp_b200.h"
 #include "zfpb_engine.h"
+#include "zfpb_serve.h"
 
 using zfpb::u32;
 using zfpb::u64;
@@ -1339,6 +1340,47 @@ extern "C" size_t zfpb_compress_batch(zfpb_batch_item* items, size_t n, void* cu
 extern "C" size_t zfpb_decompress_batch(zfpb_batch_item* items, size_t n, void* cuda_stream) {
   return run_batch_abi(items, n, cuda_stream, false);
 }
+
+// Serving loop (zfpb_serve.cpp): items converted to engine jobs at submit.
+extern "C" zfpb_server* zfpb_server_create(size_t budget_bytes, int lanes, size_t max_batch) {
+  zfpb::Server* s = zfpb::server_create(budget_bytes, lanes, max_batch);
+  if (!s) fail(zfpb::ERR_CUDA);
+  return reinterpret_cast<zfpb_server*>(s);
+}
+
+extern "C" int zfpb_server_submit(zfpb_server* srv, const zfpb_batch_item* it, int decompress, uint64_t tag) {
+  if (!srv || !it || !it->d_field || !it->d_stream || ((uintptr_t)it->d_stream % 8) != 0) return fail(zfpb::ERR_ARGS);
+  Plan p;
+  zfpb::BatchJob J{};
+  if (!call_of_desc(&it->desc, p, J.call, it->d_field)) return fail(zfpb::ERR_ARGS);
+  J.field = it->d_field;
+  J.stream = (u64*)it->d_stream;
+  J.stream_words = it->stream_bytes / 8;
+  J.index = (u64*)it->d_block_offsets;
+  if (!zfpb::server_submit(reinterpret_cast<zfpb::Server*>(srv), J, decompress != 0, tag))
+    return fail(zfpb::ERR_TOO_LARGE);
+  return 1;
+}
+
+extern "C" size_t zfpb_server_poll(zfpb_server* srv, zfpb_request_done* out, size_t max, int wait_ms) {
+  if (!srv || (!out && max)) return 0;
+  std::vector<zfpb::ServeDone> d(max);
+  size_t n = zfpb::server_poll(reinterpret_cast<zfpb::Server*>(srv), d.data(), max, wait_ms);
+  for (size_t i = 0; i < n; i++) {
+    out[i].tag = d[i].tag;
+    out[i].result = (size_t)d[i].result;
+    out[i].status = d[i].status;
+    out[i].queue_ms = d[i].queue_ms;
+    out[i].latency_ms = d[i].latency_ms;
+  }
+  return n;
+}
+
+extern "C" size_t zfpb_server_outstanding(zfpb_server* srv) {
+  return srv ? zfpb::server_outstanding(reinterpret_cast<zfpb::Server*>(srv)) : 0;
+}
+
+extern "C" void zfpb_server_destroy(zfpb_server* srv) { zfpb::server_destroy(reinterpret_cast<zfpb::Server*>(srv)); }
 
 // Same stream as zfpb_compress_device, with scratch from the library's static
 // device array instead of cudaMalloc (see include/zfp_b200.h).  Allocates

@@ -704,6 +704,25 @@ struct BatchRound {
   std::vector<std::pair<int, std::pair<u32, u32>>> walks;  // (type*8+dims, (first, count) in walk list)
 };
 
+// Pinned host memory, grown on demand.
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t need) {
+    if (need <= bytes) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    size_t grow = std::max(need, (size_t)4096);
+    cudaError_t e = cudaMallocHost(&p, grow);
+    if (e == cudaSuccess) bytes = grow;
+    return e;
+  }
+  ~PinnedBuf() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
 struct BatchPlan {
   bool compress;
   int device;
@@ -715,22 +734,30 @@ struct BatchPlan {
   std::vector<BatchRound> rounds;
   u64 max_entries = 0, max_slot_words = 0, max_cols = 0, max_walk = 0;
   Buf d_items, d_tiles, d_walk, slots, lengths, offsets, partial, flags, planes, heads, walk_planes, ends;
+  PinnedBuf h_stage, h_ends_buf, h_flags_buf;
   u64* h_ends = nullptr;
   unsigned* h_flags = nullptr;
   cudaGraphExec_t graph = nullptr;
   bool capture_tried = false;
+  void reset() {
+    items.clear();
+    job_of_item.clear();
+    tiles.clear();
+    walk.clear();
+    rounds.clear();
+    max_entries = max_slot_words = max_cols = max_walk = 0;
+  }
   ~BatchPlan() {
     if (graph) cudaGraphExecDestroy(graph);
     for (Buf* b : {&d_items, &d_tiles, &d_walk, &slots, &lengths, &offsets, &partial, &flags, &planes, &heads,
                    &walk_planes, &ends})
       if (b->p) cudaFree(b->p);
-    if (h_ends) cudaFreeHost(h_ends);
-    if (h_flags) cudaFreeHost(h_flags);
   }
 };
 
 std::mutex g_batch_mu;
 std::vector<std::unique_ptr<BatchPlan>> g_plans;  // most recently used last
+std::mutex g_tune_mu;
 std::map<int, int> g_tuned;                          // (pass, type, dims) -> threads
 
 int tune_key(int pass, int type, int dims) { return (pass * 8 + type) * 8 + dims; }
@@ -825,12 +852,18 @@ cudaError_t run_plan(BatchPlan& P, cudaStream_t s, bool tune) {
     for (BatchLaunch& L : R.launches) {
       int th = L.threads;
       if (!th) {
-        auto it = g_tuned.find(tune_key(L.pass, L.type, L.dims));
-        if (it != g_tuned.end()) {
-          th = it->second;
+        int known = 0;
+        {
+          std::lock_guard<std::mutex> l(g_tune_mu);
+          auto it = g_tuned.find(tune_key(L.pass, L.type, L.dims));
+          if (it != g_tuned.end()) known = it->second;
+        }
+        if (known) {
+          th = known;
         } else if (tune) {
           e = tune_launch(L, a, s, &th);
           if (e != cudaSuccess) return e;
+          std::lock_guard<std::mutex> l(g_tune_mu);
           g_tuned[tune_key(L.pass, L.type, L.dims)] = th;
         } else {
           th = thread_candidates(L.pass, L.type, L.dims)[0];
@@ -877,8 +910,10 @@ std::vector<char> plan_key(const BatchJob* jobs, size_t n, bool compress, int de
   return k;
 }
 
-// Build a plan for the jobs that go through the batch kernels (batched[]).
-cudaError_t build_plan(BatchPlan& P, const BatchJob* jobs, const std::vector<u32>& batched) {
+// Build a plan for the jobs that go through the batch kernels (batched[]),
+// reusing P's buffers; its tables are copied to the device on s.
+cudaError_t build_plan(BatchPlan& P, const BatchJob* jobs, const std::vector<u32>& batched, cudaStream_t s) {
+  P.reset();
   // Order items by round; within a round, by class, so a class's tiles are contiguous.
   std::vector<std::vector<u32>> rounds;
   {
@@ -1000,23 +1035,29 @@ cudaError_t build_plan(BatchPlan& P, const BatchJob* jobs, const std::vector<u32
       if ((e = P.walk_planes.ensure(256 * P.max_walk * sizeof(u64))) != cudaSuccess) return e;
     }
   }
-  if ((e = cudaMallocHost((void**)&P.h_ends, nitems * sizeof(u64))) != cudaSuccess) return e;
-  if ((e = cudaMallocHost((void**)&P.h_flags, nitems * sizeof(unsigned))) != cudaSuccess) return e;
-  if ((e = cudaMemcpy(P.d_items.p, P.items.data(), nitems * sizeof(BatchItem), cudaMemcpyHostToDevice)) !=
-      cudaSuccess)
-    return e;
-  if (!P.tiles.empty() && (e = cudaMemcpy(P.d_tiles.p, P.tiles.data(), P.tiles.size() * sizeof(BatchTile),
-                                          cudaMemcpyHostToDevice)) != cudaSuccess)
-    return e;
-  if (!P.walk.empty() &&
-      (e = cudaMemcpy(P.d_walk.p, P.walk.data(), P.walk.size() * sizeof(u32), cudaMemcpyHostToDevice)) != cudaSuccess)
-    return e;
+  if ((e = P.h_ends_buf.ensure(nitems * sizeof(u64))) != cudaSuccess) return e;
+  if ((e = P.h_flags_buf.ensure(nitems * sizeof(unsigned))) != cudaSuccess) return e;
+  P.h_ends = (u64*)P.h_ends_buf.p;
+  P.h_flags = (unsigned*)P.h_flags_buf.p;
+  // Tables through pinned staging, copied asynchronously on s.
+  const size_t bi = nitems * sizeof(BatchItem), bt = P.tiles.size() * sizeof(BatchTile),
+               bw = P.walk.size() * sizeof(u32);
+  if ((e = P.h_stage.ensure(bi + bt + bw)) != cudaSuccess) return e;
+  char* st = (char*)P.h_stage.p;
+  memcpy(st, P.items.data(), bi);
+  if (bt) memcpy(st + bi, P.tiles.data(), bt);
+  if (bw) memcpy(st + bi + bt, P.walk.data(), bw);
+  if ((e = cudaMemcpyAsync(P.d_items.p, st, bi, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  if (bt && (e = cudaMemcpyAsync(P.d_tiles.p, st + bi, bt, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  if (bw && (e = cudaMemcpyAsync(P.d_walk.p, st + bi + bt, bw, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
   return cudaSuccess;
 }
 
-// Run the jobs that the batch kernels can take, through a cached plan.
-Status run_batch(BatchJob* jobs, size_t n, bool compress, cudaStream_t s) {
-  std::vector<u32> batched, single;
+// Split jobs into those the batch kernels take and those decoded alone
+// (fields whose strides alias); empty fields are done.
+void classify(BatchJob* jobs, size_t n, bool compress, std::vector<u32>& batched, std::vector<u32>& single) {
+  batched.clear();
+  single.clear();
   for (size_t i = 0; i < n; i++) {
     BatchJob& J = jobs[i];
     J.status = OK;
@@ -1026,6 +1067,44 @@ Status run_batch(BatchJob* jobs, size_t n, bool compress, cudaStream_t s) {
     if (!compress && strides_may_alias(c.f, c.dims)) single.push_back((u32)i);
     else batched.push_back((u32)i);
   }
+}
+
+// After the plan's launches completed: each job's end bit and status; jobs
+// whose index did not match join `single` to be walked alone.
+void collect(const BatchPlan& P, BatchJob* jobs, bool compress, std::vector<u32>& single) {
+  for (size_t k = 0; k < P.items.size(); k++) {
+    BatchJob& J = jobs[P.job_of_item[k]];
+    J.end_bit = P.h_ends[k];
+    const unsigned fl = P.h_flags[k];
+    if (compress) {
+      if ((J.end_bit + 63) / 64 > J.stream_words) J.status = ERR_OVERFLOW;
+    } else if (fl & FLAG_BAD_INDEX) {
+      single.push_back(P.job_of_item[k]);
+    } else if (fl & FLAG_TRUNCATED) {
+      J.status = ERR_TRUNCATED;
+    }
+  }
+}
+
+// Jobs run alone: decompress without an index (compress never needs it).
+Status finish_jobs(BatchJob* jobs, size_t n, bool compress, const std::vector<u32>& single, cudaStream_t s) {
+  for (u32 i : single) {
+    BatchJob& J = jobs[i];
+    u64 end = 0;
+    Status st = compress ? ERR_ARGS : decompress(J.call, J.stream, J.stream_words, 0, J.field, &end, nullptr, s);
+    J.status = st;
+    J.end_bit = end;
+  }
+  Status all = OK;
+  for (size_t i = 0; i < n; i++)
+    if (jobs[i].status != OK) all = jobs[i].status;
+  return all;
+}
+
+// Run the jobs that the batch kernels can take, through a cached plan.
+Status run_batch(BatchJob* jobs, size_t n, bool compress, cudaStream_t s) {
+  std::vector<u32> batched, single;
+  classify(jobs, n, compress, batched, single);
   if (!batched.empty()) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -1051,7 +1130,7 @@ Status run_batch(BatchJob* jobs, size_t n, bool compress, cudaStream_t s) {
         np->compress = compress;
         np->device = dev;
         np->key = key;
-        if (build_plan(*np, jobs, batched) != cudaSuccess) {
+        if (build_plan(*np, jobs, batched, s) != cudaSuccess) {
           cudaGetLastError();
           return ERR_CUDA;
         }
@@ -1077,37 +1156,79 @@ Status run_batch(BatchJob* jobs, size_t n, bool compress, cudaStream_t s) {
       cudaGetLastError();
     }
     if (cudaStreamSynchronize(s) != cudaSuccess) return ERR_CUDA;
-    for (size_t k = 0; k < P->items.size(); k++) {
-      BatchJob& J = jobs[P->job_of_item[k]];
-      J.end_bit = P->h_ends[k];
-      const unsigned fl = P->h_flags[k];
-      if (compress) {
-        if ((J.end_bit + 63) / 64 > J.stream_words) J.status = ERR_OVERFLOW;
-      } else if (fl & FLAG_BAD_INDEX) {
-        single.push_back(P->job_of_item[k]);  // index does not match: walk this one alone
-      } else if (fl & FLAG_TRUNCATED) {
-        J.status = ERR_TRUNCATED;
-      }
-    }
+    collect(*P, jobs, compress, single);
   }
-  for (u32 i : single) {
-    BatchJob& J = jobs[i];
-    u64 end = 0;
-    Status st = compress ? ERR_ARGS
-                         : decompress(J.call, J.stream, J.stream_words, 0, J.field, &end, nullptr, s);
-    J.status = st;
-    J.end_bit = end;
-  }
-  Status all = OK;
-  for (size_t i = 0; i < n; i++)
-    if (jobs[i].status != OK) all = jobs[i].status;
-  return all;
+  return finish_jobs(jobs, n, compress, single, s);
 }
 
 }  // namespace
 
 Status compress_batch(BatchJob* jobs, size_t n, cudaStream_t s) { return run_batch(jobs, n, true, s); }
 Status decompress_batch(BatchJob* jobs, size_t n, cudaStream_t s) { return run_batch(jobs, n, false, s); }
+
+u64 batch_scratch_bytes(const Call& c, bool compress) {
+  const u64 n = c.f.nblocks;
+  if (compress) return n * ((block_bits(c.c, c.type, c.dims) + 63) / 64 + 1) * sizeof(u64) + (n + 1) * 12;
+  return (c.dims == 3 ? n * 65 * sizeof(u64) : 0) + (n + 1) * sizeof(u64);
+}
+
+// Asynchronous batches (the serving loop): plan on the host, launch on s,
+// return; the caller polls batch_ready and then calls batch_collect.  No
+// tuning (classes use the CTA sizes tuned so far, else 128 threads) and no
+// graph: each run is a different set of requests.
+struct BatchRun {
+  BatchPlan plan;
+  std::vector<BatchJob> jobs;
+  std::vector<u32> batched, single;
+  bool compress = true;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  bool launched = false;
+};
+
+BatchRun* batch_run_create() {
+  BatchRun* r = new BatchRun();
+  if (cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming) != cudaSuccess) {
+    delete r;
+    return nullptr;
+  }
+  return r;
+}
+
+void batch_run_destroy(BatchRun* r) {
+  if (!r) return;
+  if (r->launched) cudaEventSynchronize(r->done);
+  cudaEventDestroy(r->done);
+  delete r;
+}
+
+Status batch_launch(BatchRun* r, const BatchJob* jobs, size_t n, bool compress, cudaStream_t s) {
+  r->jobs.assign(jobs, jobs + n);
+  r->compress = compress;
+  r->stream = s;
+  r->plan.compress = compress;
+  classify(r->jobs.data(), n, compress, r->batched, r->single);
+  if (!r->batched.empty()) {
+    if (build_plan(r->plan, r->jobs.data(), r->batched, s) != cudaSuccess) return ERR_CUDA;
+    if (run_plan(r->plan, s, false) != cudaSuccess) return ERR_CUDA;
+  }
+  if (cudaEventRecord(r->done, s) != cudaSuccess) return ERR_CUDA;
+  r->launched = true;
+  return OK;
+}
+
+bool batch_ready(BatchRun* r) { return !r->launched || cudaEventQuery(r->done) != cudaErrorNotReady; }
+
+Status batch_collect(BatchRun* r, BatchJob* out) {
+  if (!r->launched) return ERR_ARGS;
+  if (cudaEventSynchronize(r->done) != cudaSuccess) return ERR_CUDA;
+  r->launched = false;
+  if (!r->batched.empty()) collect(r->plan, r->jobs.data(), r->compress, r->single);
+  Status st = finish_jobs(r->jobs.data(), r->jobs.size(), r->compress, r->single, r->stream);
+  if (!r->single.empty()) cudaStreamSynchronize(r->stream);
+  std::copy(r->jobs.begin(), r->jobs.end(), out);
+  return st;
+}
 
 }  // namespace zfpb
 

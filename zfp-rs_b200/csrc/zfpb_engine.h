@@ -176,6 +176,21 @@ struct BatchJob {
 Status compress_batch(BatchJob* jobs, size_t n, cudaStream_t s);
 Status decompress_batch(BatchJob* jobs, size_t n, cudaStream_t s);
 
+// The same, asynchronous: batch_launch plans and launches on s and returns;
+// once batch_ready, batch_collect writes every job's result to out (in the
+// order given).  A BatchRun keeps its scratch for the next launch; one run
+// at a time per BatchRun.
+struct BatchRun;
+BatchRun* batch_run_create();
+void batch_run_destroy(BatchRun* r);
+Status batch_launch(BatchRun* r, const BatchJob* jobs, size_t n, bool compress, cudaStream_t s);
+bool batch_ready(BatchRun* r);
+Status batch_collect(BatchRun* r, BatchJob* out);
+
+// Device scratch a job needs inside a batch beyond its own buffers (block
+// slots for compress, plane scratch for a 3D decompress), for admission.
+u64 batch_scratch_bytes(const Call& call, bool compress);
+
 // Kernel launchers, one instantiation per scalar type (zfpb_inst_*.cu).
 template <class T> struct Launch {
   static cudaError_t encode_fixed(const Call& call, const EncodeFixedArgs& a, u64 ctas, int threads,

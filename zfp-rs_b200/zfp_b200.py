@@ -81,6 +81,13 @@ class ZfpBatchItem(C.Structure):
                 ("d_block_offsets", C.c_void_p), ("result", C.c_size_t), ("status", C.c_int)]
 
 
+class ZfpRequestDone(C.Structure):
+    """zfpb_request_done (include/zfp_b200.h)."""
+
+    _fields_ = [("tag", C.c_uint64), ("result", C.c_size_t), ("status", C.c_int), ("queue_ms", C.c_double),
+                ("latency_ms", C.c_double)]
+
+
 # (name, restype, argtypes) of every function include/zfp.h and include/zfp_b200.h declare.
 _vp, _sz, _u, _u64, _i32, _b = C.c_void_p, C.c_size_t, C.c_uint, C.c_uint64, C.c_int32, C.c_int32
 _F = C.POINTER(ZfpField)
@@ -140,6 +147,11 @@ SIGNATURES = [
     ("zfpb_compress_device_noalloc", _sz, [C.POINTER(ZfpDesc), _vp, _vp, _sz, _vp]),
     ("zfpb_compress_batch", _sz, [C.POINTER(ZfpBatchItem), _sz, _vp]),
     ("zfpb_decompress_batch", _sz, [C.POINTER(ZfpBatchItem), _sz, _vp]),
+    ("zfpb_server_create", _vp, [_sz, C.c_int, _sz]),
+    ("zfpb_server_submit", C.c_int, [_vp, C.POINTER(ZfpBatchItem), C.c_int, C.c_uint64]),
+    ("zfpb_server_poll", _sz, [_vp, C.POINTER(ZfpRequestDone), _sz, C.c_int]),
+    ("zfpb_server_outstanding", _sz, [_vp]),
+    ("zfpb_server_destroy", None, [_vp]),
 ]
 DATA_SYMBOLS = ["stream_word_bits", "zfp_codec_version", "zfp_library_version"]
 
@@ -424,3 +436,35 @@ def decompress_batch(items, stream=None):
     if ok != len(items):
         raise ZfpError("decompress_batch", lib().zfpb_last_error())
     return [it.result for it in items]
+
+
+class Server:
+    """The serving loop (zfpb_server_*): submit requests, poll results."""
+
+    def __init__(self, budget_bytes: int, lanes: int = 2, max_batch: int = 0):
+        self.h = lib().zfpb_server_create(budget_bytes, lanes, max_batch)
+        if not self.h:
+            raise ZfpError("server_create", lib().zfpb_last_error())
+        self._keep = {}
+
+    def submit(self, item: "ZfpBatchItem", decompress: bool, tag: int) -> bool:
+        ok = lib().zfpb_server_submit(self.h, C.byref(item), int(decompress), tag)
+        if ok:
+            self._keep[tag] = item
+        return bool(ok)
+
+    def poll(self, max_n: int = 256, wait_ms: int = 0):
+        out = (ZfpRequestDone * max_n)()
+        n = lib().zfpb_server_poll(self.h, out, max_n, wait_ms)
+        res = [(d.tag, d.result, d.status, d.queue_ms, d.latency_ms) for d in out[:n]]
+        for r in res:
+            self._keep.pop(r[0], None)
+        return res
+
+    def outstanding(self) -> int:
+        return lib().zfpb_server_outstanding(self.h)
+
+    def close(self):
+        if self.h:
+            lib().zfpb_server_destroy(self.h)
+            self.h = None
