@@ -53,6 +53,15 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-fixed", action="store_true", help="skip the fixed-rate float32 measurement")
+    ap.add_argument("--batched-arrays", type=int, default=2000,
+                    help="arrays in the batched workload (0 skips it)")
+    ap.add_argument("--batched-max-elems", type=int, default=16_777_216,
+                    help="largest array of the batched workload, in elements")
+    ap.add_argument("--serve-rates", default="1000,5000",
+                    help="serving: Poisson arrival rates (req/s), comma separated; empty skips")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="serving: length of each arrival stream")
+    ap.add_argument("--serve-small-rate", type=float, default=20000.0,
+                    help="serving: rate of a stream of small requests (16 KB..1 MB); 0 skips")
     return ap.parse_args()
 
 
@@ -332,6 +341,16 @@ def main():
     # Fixed-rate 8 float32, device resident.
     fr = None if args.no_fixed else fixed_rate_measure(Z, n, dev, args, peak)
 
+    # Batched workload (2,000 mixed arrays) against one call per array.
+    del out, stream_buf
+    torch.cuda.empty_cache()
+    bt = batched_measure(Z, dev, args) if args.batched_arrays > 0 else None
+    rates = [float(r) for r in args.serve_rates.split(",") if r.strip()]
+    sv = [serving_measure(Z, dev, args, r) for r in rates]
+    if args.serve_small_rate > 0:
+        sv.append(serving_measure(Z, dev, args, args.serve_small_rate, max_bytes=1 << 20))
+    sv = sv or None
+
     if rank == 0:
         line = {
             "metric": "compress/decompress GB/s on 1 B200 (bit-exact); batched p50/p99 ms",
@@ -348,6 +367,8 @@ def main():
             "gpu_launches": launches,
             "e2e": e2e,
             "fixed_rate_f32": fr,
+            "batched": bt,
+            "serving": sv,
             "clocks": clock_info,
         }
         if ws == 1 and not args.no_cpu:
@@ -355,6 +376,256 @@ def main():
         print(json.dumps(line))
     if pg is not None:
         pg.destroy_process_group()
+
+
+def batched_workload(n_arrays, max_elems, dev, seed=0):
+    """2,000 arrays: 60% float32, 30% float64, 10% int32; 1D/2D/3D; element
+    counts log-uniform from 64 to max_elems, no side a multiple of 4; per-array
+    fixed-rate 2-32, fixed-precision 8-48 or fixed-accuracy 1e-2..1e-9 and a
+    random rounding; values sin(0.10x)cos(0.13y)sin(0.07z) + N(0, 1e-3) with
+    seed i (int32: scaled by 2^20).  Synthetic, seeded."""
+    import torch
+
+    from tests import zfpb
+
+    Z = zfpb.load()
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for i in range(n_arrays):
+        u = rng.random()
+        dtype = np.float32 if u < 0.6 else (np.float64 if u < 0.9 else np.int32)
+        dims = int(rng.integers(1, 4))
+        n = float(np.exp(rng.uniform(np.log(64), np.log(max_elems))))
+        base = n ** (1.0 / dims)
+        shape = []
+        for _ in range(dims):
+            side = max(1, int(round(base * rng.uniform(0.8, 1.25))))
+            if side % 4 == 0:
+                side += 1
+            shape.append(side)
+        g = torch.Generator(device=dev)
+        g.manual_seed(seed * 100003 + i)
+        freqs = [0.10, 0.13, 0.07]
+        funcs = [torch.sin, torch.cos, torch.sin]
+        f = torch.ones(shape, device=dev, dtype=torch.float64)
+        for ax in range(dims):  # x is the last (fastest) axis
+            c = torch.arange(shape[dims - 1 - ax], device=dev, dtype=torch.float64)
+            v = funcs[ax](freqs[ax] * c)
+            view = [1] * dims
+            view[dims - 1 - ax] = -1
+            f = f * v.view(view)
+        f = f + 1e-3 * torch.randn(shape, generator=g, device=dev, dtype=torch.float64)
+        if dtype == np.int32:
+            x = torch.round(f * 2 ** 20).to(torch.int32)
+        else:
+            x = f.to(torch.float32 if dtype == np.float32 else torch.float64)
+        kinds = 3 if dtype != np.int32 else 2
+        k = int(rng.integers(0, kinds))
+        if k == 0:
+            cfg = Z.ZfpConfig.fixed_rate(float(rng.integers(2, 33)), dtype, dims)
+        elif k == 1:
+            cfg = Z.ZfpConfig.fixed_precision(int(rng.integers(8, 49)))
+        else:
+            cfg = Z.ZfpConfig.fixed_accuracy(float(10.0 ** -rng.uniform(2, 9)))
+        cfg = cfg.with_rounding(["never", "first", "last"][int(rng.integers(0, 3))], bool(rng.integers(0, 2)))
+        jobs.append((x, cfg))
+    return jobs
+
+
+def batched_measure(Z, dev, args):
+    """Batched workload through zfpb_compress_batch / zfpb_decompress_batch
+    (one plan, replayed as a CUDA graph) against one zfpb_compress_device /
+    zfpb_decompress_device call per array, same output checked bit for bit."""
+    import torch
+
+    jobs = batched_workload(args.batched_arrays, args.batched_max_elems, dev)
+    fields = [x for x, _ in jobs]
+    cfgs = [c for _, c in jobs]
+    total = sum(x.numel() * x.element_size() for x in fields)
+    caps = [Z.maximum_size(x.shape, Z._np_dtype(x.dtype), c) for x, c in jobs]
+    streams = [torch.empty((cap + 7) // 8, dtype=torch.int64, device=dev) for cap in caps]
+    offs = [torch.empty(int(np.prod([(n + 3) // 4 for n in x.shape])) + 1, dtype=torch.int64, device=dev)
+            for x in fields]
+    outs = [torch.empty_like(x) for x in fields]
+    citems = Z.batch_items(fields, cfgs, streams, offsets=offs)
+    sizes = Z.compress_batch(citems)  # plans, tunes, captures
+    sizes = Z.compress_batch(citems)
+    ditems = Z.batch_items(outs, cfgs, streams, nbytes=sizes, offsets=offs)
+    Z.decompress_batch(ditems)
+    Z.decompress_batch(ditems)
+    cs = torch.cuda.current_stream(dev)
+    reps = max(5, args.steps)
+
+    def timed(fn, n):
+        ts = []
+        for _ in range(n):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            e0.record(cs)
+            fn()
+            e1.record(cs)
+            torch.cuda.synchronize(dev)
+            ts.append(e0.elapsed_time(e1))
+        return ts
+
+    bc = timed(lambda: Z.compress_batch(citems), reps)
+    bd = timed(lambda: Z.decompress_batch(ditems), reps)
+    # One call per array, the plain GPU form, into separate buffers.
+    s2 = [torch.empty_like(s) for s in streams]
+    o2 = [torch.empty_like(x) for x in fields]
+    single_sizes = [0] * len(jobs)
+
+    def per_array_compress():
+        for i, (x, c) in enumerate(jobs):
+            single_sizes[i] = Z.compress_device(x, c, out=s2[i], offsets=offs[i])
+
+    def per_array_decompress():
+        for i, (x, c) in enumerate(jobs):
+            Z.decompress_device(s2[i], single_sizes[i], o2[i], c, offsets=offs[i])
+
+    per_array_compress()
+    per_array_decompress()
+    sc = timed(per_array_compress, 2)
+    sd = timed(per_array_decompress, 2)
+    same = all(sizes[i] == single_sizes[i] and torch.equal(streams[i][: sizes[i] // 8], s2[i][: sizes[i] // 8])
+               and torch.equal(outs[i].view(torch.uint8), o2[i].view(torch.uint8)) for i in range(len(jobs)))
+    p = lambda v, q: float(np.percentile(v, q))
+    res = {
+        "workload": f"{len(jobs)} arrays, 60% f32 / 30% f64 / 10% i32, 1D-3D, 64..{args.batched_max_elems} elements "
+                    f"log-uniform, sides not multiples of 4, per-array fixed-rate 2-32 / fixed-precision 8-48 / "
+                    f"fixed-accuracy 1e-2..1e-9, random rounding",
+        "arrays": len(jobs), "bytes": total, "stream_bytes": int(sum(sizes)),
+        "compress_ms_p50": p(bc, 50), "compress_ms_p99": p(bc, 99),
+        "decompress_ms_p50": p(bd, 50), "decompress_ms_p99": p(bd, 99),
+        "compress_gbs": total / (p(bc, 50) / 1e3) / 1e9, "decompress_gbs": total / (p(bd, 50) / 1e3) / 1e9,
+        "per_array_compress_ms": min(sc), "per_array_decompress_ms": min(sd),
+        "speedup_compress": min(sc) / p(bc, 50), "speedup_decompress": min(sd) / p(bd, 50),
+        "identical_to_per_array": bool(same), "reps": reps,
+        "timing": "CUDA events on the calling stream around each whole call (host planning, graph launch, "
+                  "per-array launches and synchronisations included)",
+    }
+    del streams, s2, outs, o2, fields, jobs
+    torch.cuda.empty_cache()
+    return res
+
+
+def serving_measure(Z, dev, args, rate, seed=7, max_bytes=256 << 20):
+    """Open-loop Poisson requests, 70% decompress / 30% compress, sizes
+    log-uniform 16 KB..256 MB of float32/float64 2D/3D data with the batched
+    workload's mode mix; through the serving loop (40 GB admission budget,
+    4 lanes, 64 MiB batches) and through one synchronous device call per request, on the same
+    arrival times.  Requests draw from a pool of resident arrays (requests on
+    the same array write the same bytes to its output buffers); a decompress
+    request carries its stream's block index, kept from its compression."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    pool = []
+    for i in range(48):
+        nbytes = float(np.exp(rng.uniform(np.log(16 << 10), np.log(max_bytes))))
+        dtype = np.float32 if rng.random() < 0.6 else np.float64
+        dims = int(rng.integers(2, 4))
+        n = nbytes / np.dtype(dtype).itemsize
+        base = n ** (1.0 / dims)
+        shape = [max(1, int(round(base * rng.uniform(0.8, 1.25)))) for _ in range(dims)]
+        noise = torch.randn(shape, device=dev, dtype=torch.float64) * 1e-3
+        grid = [torch.arange(m, device=dev, dtype=torch.float64) for m in shape]
+        f = torch.ones(shape, device=dev, dtype=torch.float64)
+        for ax, (fr, fn) in enumerate(zip([0.10, 0.13, 0.07], [torch.sin, torch.cos, torch.sin])):
+            if ax >= dims:
+                break
+            view = [1] * dims
+            view[dims - 1 - ax] = -1
+            f = f * fn(fr * grid[dims - 1 - ax]).view(view)
+        x = (f + noise).to(torch.float32 if dtype == np.float32 else torch.float64)
+        k = int(rng.integers(0, 3))
+        if k == 0:
+            cfg = Z.ZfpConfig.fixed_rate(float(rng.integers(2, 33)), dtype, dims)
+        elif k == 1:
+            cfg = Z.ZfpConfig.fixed_precision(int(rng.integers(8, 49)))
+        else:
+            cfg = Z.ZfpConfig.fixed_accuracy(float(10.0 ** -rng.uniform(2, 9)))
+        cfg = cfg.with_rounding(["never", "first", "last"][int(rng.integers(0, 3))], bool(rng.integers(0, 2)))
+        cap = Z.maximum_size(x.shape, dtype, cfg)
+        stream = torch.empty((cap + 7) // 8, dtype=torch.int64, device=dev)
+        index = torch.empty(int(np.prod([(m + 3) // 4 for m in shape])) + 1, dtype=torch.int64, device=dev)
+        nb = Z.compress_device(x, cfg, out=stream, offsets=index)  # the stream's block index is kept with it
+        cstream = torch.empty_like(stream)
+        out = torch.empty_like(x)
+        citem = Z.batch_items([x], [cfg], [cstream])[0]
+        ditem = Z.batch_items([out], [cfg], [stream], nbytes=[nb], offsets=[index])[0]
+        pool.append(dict(x=x, cfg=cfg, stream=stream, nb=nb, index=index, cstream=cstream, out=out, citem=citem,
+                         ditem=ditem, bytes=x.numel() * x.element_size()))
+    nreq = int(rate * args.serve_seconds)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
+    which = rng.integers(0, len(pool), size=nreq)
+    dec = rng.random(nreq) < 0.7
+    total = sum(pool[w]["bytes"] for w in which)
+    torch.cuda.synchronize(dev)
+
+    # Serving loop, warmed with one request per pool array of each kind (its
+    # lanes' scratch grows to size), then timed.
+    server = Z.Server(40 << 30)
+    for j, e in enumerate(pool):
+        assert server.submit(e["citem"], False, 2 * j) and server.submit(e["ditem"], True, 2 * j + 1)
+    warm = 0
+    while warm < 2 * len(pool):
+        warm += len(server.poll(256, wait_ms=20))
+    lat = np.zeros(nreq)
+    queue = np.zeros(nreq)
+    got = 0
+    bad = 0
+    t0 = time.perf_counter()
+    for i in range(nreq):
+        while time.perf_counter() - t0 < arrivals[i]:
+            for tag, res, st, q, l in server.poll(256, wait_ms=0):
+                lat[tag], queue[tag] = l, q
+                got += 1
+                bad += st != 0
+        e = pool[which[i]]
+        assert server.submit(e["ditem"] if dec[i] else e["citem"], bool(dec[i]), i)
+    while got < nreq:
+        for tag, res, st, q, l in server.poll(256, wait_ms=20):
+            lat[tag], queue[tag] = l, q
+            got += 1
+            bad += st != 0
+    t_serve = time.perf_counter() - t0
+    server.close()
+
+    # One synchronous device call per request, same arrival times (warmed the
+    # same way: its workspace grows to size first).
+    for e in pool:
+        Z.compress_device(e["x"], e["cfg"], out=e["cstream"])
+        Z.decompress_device(e["stream"], e["nb"], e["out"], e["cfg"], offsets=e["index"])
+    torch.cuda.synchronize(dev)
+    lat1 = np.zeros(nreq)
+    t0 = time.perf_counter()
+    for i in range(nreq):
+        while time.perf_counter() - t0 < arrivals[i]:
+            pass
+        e = pool[which[i]]
+        if dec[i]:
+            Z.decompress_device(e["stream"], e["nb"], e["out"], e["cfg"], offsets=e["index"])
+        else:
+            Z.compress_device(e["x"], e["cfg"], out=e["cstream"])
+        lat1[i] = (time.perf_counter() - t0 - arrivals[i]) * 1e3
+    t_single = time.perf_counter() - t0
+    pct = lambda v, q: float(np.percentile(v, q))
+    res = {
+        "workload": f"Poisson {rate:g} req/s for {args.serve_seconds:g} s, 70% decompress / 30% compress, "
+                    f"16 KB..{max_bytes >> 20} MB float32/float64 2D/3D, batched mode mix, 40 GB admission budget, "
+                    f"4 lanes, 64 MiB batches",
+        "requests": nreq, "bytes": int(total),
+        "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "gbs": total / t_serve / 1e9, "wall_s": t_serve,
+        "queue_p50_ms": pct(queue, 50), "queue_p99_ms": pct(queue, 99), "failed": int(bad),
+        "per_request_p50_ms": pct(lat1, 50), "per_request_p99_ms": pct(lat1, 99),
+        "per_request_gbs": total / t_single / 1e9, "per_request_wall_s": t_single,
+        "timing": "latency = submit to result on the host (wall clock); throughput = request bytes / wall time "
+                  "from the first arrival to the last result",
+    }
+    del pool
+    torch.cuda.empty_cache()
+    return res
 
 
 def traffic_of(kind):

@@ -126,9 +126,10 @@ typedef struct zfpb_request_done {
 } zfpb_request_done;
 
 /* budget_bytes: device memory that admitted requests may hold at once;
- * lanes: batches in flight at once (0: 2); max_batch: requests per batch
- * (0: no limit but 4096).  Returns NULL on failure. */
-zfpb_server* zfpb_server_create(size_t budget_bytes, int lanes, size_t max_batch);
+ * lanes: batches in flight at once (0: 4); max_batch: requests per batch
+ * (0: 4096); batch_bytes: uncompressed bytes per batch, a larger request
+ * running alone (0: 64 MiB).  Returns NULL on failure. */
+zfpb_server* zfpb_server_create(size_t budget_bytes, int lanes, size_t max_batch, size_t batch_bytes);
 /* Queue one request (decompress = 0: compress item->d_field into
  * item->d_stream).  Returns 0 if the request is invalid or alone exceeds the
  * budget. */

@@ -1342,8 +1342,8 @@ extern "C" size_t zfpb_decompress_batch(zfpb_batch_item* items, size_t n, void* 
 }
 
 // Serving loop (zfpb_serve.cpp): items converted to engine jobs at submit.
-extern "C" zfpb_server* zfpb_server_create(size_t budget_bytes, int lanes, size_t max_batch) {
-  zfpb::Server* s = zfpb::server_create(budget_bytes, lanes, max_batch);
+extern "C" zfpb_server* zfpb_server_create(size_t budget_bytes, int lanes, size_t max_batch, size_t batch_bytes) {
+  zfpb::Server* s = zfpb::server_create(budget_bytes, lanes, max_batch, batch_bytes);
   if (!s) fail(zfpb::ERR_CUDA);
   return reinterpret_cast<zfpb_server*>(s);
 }

@@ -332,6 +332,7 @@ __global__ void __launch_bounds__(256) k_pack(PackArgs a) {
 struct Buf {
   void* p = nullptr;
   size_t bytes = 0;
+  cudaStream_t owner = nullptr;  // set: allocated stream-ordered on this stream
   cudaError_t ensure(size_t need) {
     if (need <= bytes) return cudaSuccess;
     if (p) cudaFree(p);
@@ -341,6 +342,28 @@ struct Buf {
     cudaError_t e = cudaMalloc(&p, grow);
     if (e == cudaSuccess) bytes = grow;
     return e;
+  }
+  // Grow in stream order on s from `pool` (no device-wide synchronisation),
+  // by 1.5x steps.
+  cudaError_t ensure_on(size_t need, cudaStream_t s, cudaMemPool_t pool) {
+    if (need <= bytes) return cudaSuccess;
+    if (p) cudaFreeAsync(p, owner);
+    p = nullptr;
+    bytes = 0;
+    size_t grow = std::max(need + need / 2, (size_t)1 << 16);
+    cudaError_t e = cudaMallocFromPoolAsync(&p, grow, pool, s);
+    if (e == cudaSuccess) {
+      bytes = grow;
+      owner = s;
+    }
+    return e;
+  }
+  void release() {
+    if (!p) return;
+    if (owner) cudaFreeAsync(p, owner);
+    else cudaFree(p);
+    p = nullptr;
+    bytes = 0;
   }
 };
 
@@ -739,6 +762,7 @@ struct BatchPlan {
   unsigned* h_flags = nullptr;
   cudaGraphExec_t graph = nullptr;
   bool capture_tried = false;
+  cudaMemPool_t pool = nullptr;  // set: device buffers grow stream-ordered from this pool
   void reset() {
     items.clear();
     job_of_item.clear();
@@ -751,7 +775,7 @@ struct BatchPlan {
     if (graph) cudaGraphExecDestroy(graph);
     for (Buf* b : {&d_items, &d_tiles, &d_walk, &slots, &lengths, &offsets, &partial, &flags, &planes, &heads,
                    &walk_planes, &ends})
-      if (b->p) cudaFree(b->p);
+      b->release();
   }
 };
 
@@ -914,6 +938,7 @@ std::vector<char> plan_key(const BatchJob* jobs, size_t n, bool compress, int de
 // reusing P's buffers; its tables are copied to the device on s.
 cudaError_t build_plan(BatchPlan& P, const BatchJob* jobs, const std::vector<u32>& batched, cudaStream_t s) {
   P.reset();
+  auto grow = [&](Buf& b, size_t need) { return P.pool ? b.ensure_on(need, s, P.pool) : b.ensure(need); };
   // Order items by round; within a round, by class, so a class's tiles are contiguous.
   std::vector<std::vector<u32>> rounds;
   {
@@ -1015,24 +1040,24 @@ cudaError_t build_plan(BatchPlan& P, const BatchJob* jobs, const std::vector<u32
   }
   const u64 nitems = P.items.size();
   cudaError_t e;
-  if ((e = P.d_items.ensure(nitems * sizeof(BatchItem))) != cudaSuccess) return e;
-  if ((e = P.d_tiles.ensure(std::max<size_t>(1, P.tiles.size()) * sizeof(BatchTile))) != cudaSuccess) return e;
-  if ((e = P.flags.ensure(nitems * sizeof(unsigned))) != cudaSuccess) return e;
-  if ((e = P.ends.ensure(nitems * sizeof(u64))) != cudaSuccess) return e;
-  if ((e = P.offsets.ensure((P.max_entries + 1) * sizeof(u64))) != cudaSuccess) return e;
+  if ((e = grow(P.d_items, nitems * sizeof(BatchItem))) != cudaSuccess) return e;
+  if ((e = grow(P.d_tiles, std::max<size_t>(1, P.tiles.size()) * sizeof(BatchTile))) != cudaSuccess) return e;
+  if ((e = grow(P.flags, nitems * sizeof(unsigned))) != cudaSuccess) return e;
+  if ((e = grow(P.ends, nitems * sizeof(u64))) != cudaSuccess) return e;
+  if ((e = grow(P.offsets, (P.max_entries + 1) * sizeof(u64))) != cudaSuccess) return e;
   if (P.compress) {
-    if ((e = P.slots.ensure((P.max_slot_words + 1) * sizeof(u64))) != cudaSuccess) return e;
-    if ((e = P.lengths.ensure((P.max_entries + 1) * sizeof(u32))) != cudaSuccess) return e;
-    if ((e = P.partial.ensure(((P.max_entries + SCAN_TILE - 1) / SCAN_TILE + 1) * sizeof(u64))) != cudaSuccess)
+    if ((e = grow(P.slots, (P.max_slot_words + 1) * sizeof(u64))) != cudaSuccess) return e;
+    if ((e = grow(P.lengths, (P.max_entries + 1) * sizeof(u32))) != cudaSuccess) return e;
+    if ((e = grow(P.partial, ((P.max_entries + SCAN_TILE - 1) / SCAN_TILE + 1) * sizeof(u64))) != cudaSuccess)
       return e;
   } else {
     if (P.max_cols) {
-      if ((e = P.planes.ensure(64 * P.max_cols * sizeof(u64))) != cudaSuccess) return e;
-      if ((e = P.heads.ensure(P.max_cols * sizeof(u64))) != cudaSuccess) return e;
+      if ((e = grow(P.planes, 64 * P.max_cols * sizeof(u64))) != cudaSuccess) return e;
+      if ((e = grow(P.heads, P.max_cols * sizeof(u64))) != cudaSuccess) return e;
     }
     if (!P.walk.empty()) {
-      if ((e = P.d_walk.ensure(P.walk.size() * sizeof(u32))) != cudaSuccess) return e;
-      if ((e = P.walk_planes.ensure(256 * P.max_walk * sizeof(u64))) != cudaSuccess) return e;
+      if ((e = grow(P.d_walk, P.walk.size() * sizeof(u32))) != cudaSuccess) return e;
+      if ((e = grow(P.walk_planes, 256 * P.max_walk * sizeof(u64))) != cudaSuccess) return e;
     }
   }
   if ((e = P.h_ends_buf.ensure(nitems * sizeof(u64))) != cudaSuccess) return e;
@@ -1186,8 +1211,50 @@ struct BatchRun {
   bool launched = false;
 };
 
+// The memory pool of asynchronous batch scratch, one per device: it keeps
+// what it has mapped (release threshold at its maximum), so scratch that a
+// run frees and the next run takes again is not unmapped and mapped anew.
+static cudaMemPool_t batch_pool() {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> l(mu);
+  auto it = pools.find(dev);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+  unsigned long long keep = ~0ull;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  pools[dev] = pool;
+  return pool;
+}
+
+bool batch_reserve(u64 bytes, cudaStream_t s) {
+  cudaMemPool_t pool = batch_pool();
+  void* p = nullptr;
+  if (!pool || cudaMallocFromPoolAsync(&p, bytes, pool, s) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return cudaFreeAsync(p, s) == cudaSuccess;
+}
+
 BatchRun* batch_run_create() {
   BatchRun* r = new BatchRun();
+  r->plan.pool = batch_pool();
+  if (!r->plan.pool) {
+    delete r;
+    return nullptr;
+  }
+  r->plan.h_stage.ensure(1 << 20);
+  r->plan.h_ends_buf.ensure(1 << 16);
+  r->plan.h_flags_buf.ensure(1 << 16);
   if (cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming) != cudaSuccess) {
     delete r;
     return nullptr;
@@ -1198,6 +1265,7 @@ BatchRun* batch_run_create() {
 void batch_run_destroy(BatchRun* r) {
   if (!r) return;
   if (r->launched) cudaEventSynchronize(r->done);
+  if (r->stream) cudaStreamSynchronize(r->stream);
   cudaEventDestroy(r->done);
   delete r;
 }

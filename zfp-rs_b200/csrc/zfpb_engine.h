@@ -185,6 +185,8 @@ BatchRun* batch_run_create();
 void batch_run_destroy(BatchRun* r);
 Status batch_launch(BatchRun* r, const BatchJob* jobs, size_t n, bool compress, cudaStream_t s);
 bool batch_ready(BatchRun* r);
+// Map `bytes` of batch scratch ahead of use (kept by the scratch pool).
+bool batch_reserve(u64 bytes, cudaStream_t s);
 Status batch_collect(BatchRun* r, BatchJob* out);
 
 // Device scratch a job needs inside a batch beyond its own buffers (block

@@ -9,6 +9,7 @@
 // batches already in flight.  Each request's result is that of the
 // single-array device call: a batch computes every array independently.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -37,6 +38,7 @@ struct ServeRequest {
   bool decompress;
   BatchJob job;
   u64 cost;
+  u64 bytes;  // uncompressed bytes
   double t_submit, t_start;
 };
 
@@ -53,6 +55,7 @@ struct ServeLane {
 struct Server {
   u64 budget, in_use = 0;
   size_t max_batch;
+  u64 batch_bytes;
   std::vector<ServeLane> lanes;
   std::deque<ServeRequest> waiting;   // submitted, not admitted
   std::deque<ServeRequest> admitted;  // admitted, not launched
@@ -90,12 +93,18 @@ std::vector<ServeLane*> Server::admit() {
   }
   for (ServeLane& L : lanes) {
     if (L.busy || admitted.empty()) continue;
+    // The oldest request's kind; then, in arrival order, requests of that
+    // kind while the batch stays under batch_bytes of data (a larger request
+    // runs alone), so that small requests are not held behind large ones.
     const bool dec = admitted.front().decompress;
     L.reqs.clear();
+    u64 bytes = 0;
     for (auto it = admitted.begin(); it != admitted.end() && L.reqs.size() < max_batch;) {
-      if (it->decompress == dec) {
+      if (it->decompress == dec && (L.reqs.empty() || bytes + it->bytes <= batch_bytes)) {
+        bytes += it->bytes;
         L.reqs.push_back(*it);
         it = admitted.erase(it);
+        if (bytes >= batch_bytes) break;
       } else {
         ++it;
       }
@@ -161,21 +170,53 @@ void Server::loop() {
       lk.lock();
       continue;
     }
-    cv.wait(lk);
+    // Nothing to launch.  While batches are in flight, poll their events for
+    // a short while (a stream callback also wakes the loop, later); when idle,
+    // sleep until a submit or a callback.
+    const bool inflight = std::any_of(lanes.begin(), lanes.end(), [](const ServeLane& L) { return L.busy; });
+    if (inflight) {
+      lk.unlock();
+      const double until = now_s() + 200e-6;
+      bool ready = false;
+      while (!ready && now_s() < until) {
+        for (ServeLane& L : lanes)
+          if (L.busy && batch_ready(L.run)) ready = true;
+        if (!ready) std::this_thread::yield();
+      }
+      lk.lock();
+      if (ready) {
+        for (ServeLane& L : lanes)
+          if (L.busy && L.launch_ok && batch_ready(L.run)) L.finished = true;
+        continue;
+      }
+    }
+    if (!waiting.empty() || !admitted.empty()) {
+      bool idle = std::any_of(lanes.begin(), lanes.end(), [](const ServeLane& L) { return !L.busy; });
+      if (idle && !admitted.empty()) continue;
+    }
+    cv.wait_for(lk, std::chrono::milliseconds(1));
   }
 }
 
-Server* server_create(u64 budget, int nlanes, size_t max_batch) {
+Server* server_create(u64 budget, int nlanes, size_t max_batch, u64 batch_bytes) {
   Server* s = new Server();
   s->budget = budget;
   s->max_batch = max_batch ? max_batch : 4096;
+  s->batch_bytes = batch_bytes ? batch_bytes : (64ull << 20);
   cudaGetDevice(&s->device);
-  s->lanes.resize(nlanes > 0 ? nlanes : 2);
+  s->lanes.resize(nlanes > 0 ? nlanes : 4);
   for (ServeLane& L : s->lanes) {
     if (cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking) != cudaSuccess || !(L.run = batch_run_create())) {
       server_destroy(s);
       return nullptr;
     }
+  }
+  // Map scratch for the lanes up front (the pool keeps it once freed), so the
+  // first large batches do not wait for memory to be mapped.
+  if (!s->lanes.empty()) {
+    const u64 reserve = std::min<u64>(budget / 4, 6ull << 30);
+    cudaStream_t st = s->lanes[0].stream;
+    if (reserve && batch_reserve(reserve, st)) cudaStreamSynchronize(st);
   }
   s->worker = std::thread([s] { s->loop(); });
   return s;
@@ -189,7 +230,8 @@ bool server_submit(Server* s, const BatchJob& job, bool decompress, u64 tag) {
   const u64 elem = (job.call.type == 1 || job.call.type == 3) ? 4 : 8;
   u64 values = 1;
   for (int d = 0; d < job.call.dims; d++) values *= job.call.f.n[d];
-  r.cost = values * elem + job.stream_words * 8 + batch_scratch_bytes(job.call, !decompress);
+  r.bytes = values * elem;
+  r.cost = r.bytes + job.stream_words * 8 + batch_scratch_bytes(job.call, !decompress);
   if (r.cost > s->budget) return false;
   r.t_submit = now_s();
   r.t_start = 0;

@@ -17,9 +17,10 @@ struct ServeDone {
 };
 
 // budget: device bytes that admitted requests may hold at once (their fields,
-// streams and batch scratch); lanes: batches in flight at once; max_batch:
-// requests per batch (0: no limit but 4096).
-Server* server_create(u64 budget, int lanes, size_t max_batch);
+// streams and batch scratch); lanes: batches in flight at once (0: 4);
+// max_batch: requests per batch (0: 4096); batch_bytes: uncompressed bytes
+// per batch, a larger request running alone (0: 64 MiB).
+Server* server_create(u64 budget, int lanes, size_t max_batch, u64 batch_bytes);
 // false when the request alone exceeds the budget.
 bool server_submit(Server* s, const BatchJob& job, bool decompress, u64 tag);
 // Finished requests (up to max), waiting up to wait_ms for the first.

@@ -147,7 +147,7 @@ SIGNATURES = [
     ("zfpb_compress_device_noalloc", _sz, [C.POINTER(ZfpDesc), _vp, _vp, _sz, _vp]),
     ("zfpb_compress_batch", _sz, [C.POINTER(ZfpBatchItem), _sz, _vp]),
     ("zfpb_decompress_batch", _sz, [C.POINTER(ZfpBatchItem), _sz, _vp]),
-    ("zfpb_server_create", _vp, [_sz, C.c_int, _sz]),
+    ("zfpb_server_create", _vp, [_sz, C.c_int, _sz, _sz]),
     ("zfpb_server_submit", C.c_int, [_vp, C.POINTER(ZfpBatchItem), C.c_int, C.c_uint64]),
     ("zfpb_server_poll", _sz, [_vp, C.POINTER(ZfpRequestDone), _sz, C.c_int]),
     ("zfpb_server_outstanding", _sz, [_vp]),
@@ -441,8 +441,8 @@ def decompress_batch(items, stream=None):
 class Server:
     """The serving loop (zfpb_server_*): submit requests, poll results."""
 
-    def __init__(self, budget_bytes: int, lanes: int = 2, max_batch: int = 0):
-        self.h = lib().zfpb_server_create(budget_bytes, lanes, max_batch)
+    def __init__(self, budget_bytes: int, lanes: int = 0, max_batch: int = 0, batch_bytes: int = 0):
+        self.h = lib().zfpb_server_create(budget_bytes, lanes, max_batch, batch_bytes)
         if not self.h:
             raise ZfpError("server_create", lib().zfpb_last_error())
         self._keep = {}
