@@ -1068,6 +1068,9 @@ bool index_matches(const IndexCache& ix, u64 start, const zfpb::Call& call) {
          ix.c.tight == call.c.tight;
 }
 
+// Host fields from this size on go through the pipelined copy paths.
+constexpr size_t kPipelineBytes = 32u << 20;
+
 int fail(int code) {
   g_last_error = code;
   return 0;
@@ -1085,12 +1088,16 @@ extern "C" size_t zfp_compress(zfp_stream* zs, const zfp_field* f) {
   std::lock_guard<std::mutex> lock(g_abi_mu);
   cudaStream_t s = lib_stream();
 
-  // Field: device pointer as is, host span staged.
+  // Field: device pointer as is, host span staged.  A large host field with
+  // natural strides into a host stream goes through the pipelined path, which
+  // copies the field in chunk by chunk itself.
   const void* d_origin = f->data;
+  const bool pipelined = !is_device_ptr(f->data) && !zs->stream->device && p.contiguous &&
+                         p.span_bytes >= kPipelineBytes;
   if (!is_device_ptr(f->data)) {
     if (!g_field_stage.ensure(p.span_bytes)) return fail(zfpb::ERR_CUDA);
     const char* begin = (const char*)f->data + p.imin * (ptrdiff_t)es;
-    if (cudaMemcpyAsync(g_field_stage.p, begin, p.span_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    if (!pipelined && cudaMemcpyAsync(g_field_stage.p, begin, p.span_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
       return fail(zfpb::ERR_CUDA);
     d_origin = (const char*)g_field_stage.p - p.imin * (ptrdiff_t)es;
   }
@@ -1129,7 +1136,18 @@ extern "C" size_t zfp_compress(zfp_stream* zs, const zfp_field* f) {
     d_off = ix.d_off;
   }
   u64 end_rel = 0;
-  zfpb::Status st = zfpb::compress(call, d_origin, d_out, cap, start % 64, init, &end_rel, d_off, s);
+  zfpb::Status st = zfpb::ERR_ARGS;
+  if (pipelined) {
+    // Copies in and out overlap the coding, chunk by chunk.
+    st = zfpb::compress_host(call, (const char*)f->data, (void*)d_origin, bs->words + w0, d_out, cap, start % 64, init,
+                             &end_rel, d_off, s);
+  }
+  bool copied = pipelined && st != zfpb::ERR_ARGS;
+  if (!copied) {
+    if (pipelined && cudaMemcpyAsync(g_field_stage.p, f->data, p.span_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return fail(zfpb::ERR_CUDA);
+    st = zfpb::compress(call, d_origin, d_out, cap, start % 64, init, &end_rel, d_off, s);
+  }
   if (st == zfpb::ERR_OVERFLOW) {
     bs->overflowed = true;
     return fail(zfpb::ERR_OVERFLOW);
@@ -1137,7 +1155,7 @@ extern "C" size_t zfp_compress(zfp_stream* zs, const zfp_field* f) {
   if (st != zfpb::OK) return fail(st);
   const u64 end = w0 * 64 + end_rel;
   const u64 wend = (end + 63) / 64;
-  if (!bs->device && wend > w0) {
+  if (!copied && !bs->device && wend > w0) {
     if (cudaMemcpyAsync(bs->words + w0, d_out, (wend - w0) * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess)
       return fail(zfpb::ERR_CUDA);
   }
@@ -1171,6 +1189,7 @@ extern "C" size_t zfp_decompress(zfp_stream* zs, zfp_field* f) {
   const bool host_field = !is_device_ptr(f->data);
   void* d_origin = f->data;
   char* begin = (char*)f->data + p.imin * (ptrdiff_t)es;
+  const bool pipelined = host_field && !bs->device && p.contiguous && p.span_bytes >= kPipelineBytes;
   if (host_field) {
     if (!g_field_stage.ensure(p.span_bytes)) return fail(zfpb::ERR_CUDA);
     // Gaps between strided elements keep their values.
@@ -1205,13 +1224,32 @@ extern "C" size_t zfp_decompress(zfp_stream* zs, zfp_field* f) {
       need = words < avail ? words : avail;
     }
     if (!g_stream_stage.ensure((avail + 1) * 8)) return fail(zfpb::ERR_CUDA);
-    if (need && cudaMemcpyAsync(g_stream_stage.p, bs->words + w0, need * 8, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    const bool chunked = pipelined && (zfpb::fixed_size_blocks(call) || index_matches(bs->index, start, call));
+    if (!chunked && need &&
+        cudaMemcpyAsync(g_stream_stage.p, bs->words + w0, need * 8, cudaMemcpyHostToDevice, s) != cudaSuccess)
       return fail(zfpb::ERR_CUDA);
     d_in = (const u64*)g_stream_stage.p;
   }
   const u64* cand = index_matches(bs->index, start, call) ? bs->index.d_off : nullptr;
   u64 end_rel = 0;
-  zfpb::Status st = zfpb::decompress(call, d_in, avail, start % 64, d_origin, &end_rel, cand, s);
+  zfpb::Status st = zfpb::ERR_ARGS;
+  bool done_host = false;
+  if (pipelined && (cand || zfpb::fixed_size_blocks(call))) {
+    // Copies in and out overlap the decoding, chunk by chunk.
+    st = zfpb::decompress_host(call, bs->words + w0, (u64*)g_stream_stage.p, avail, start % 64, begin,
+                               (void*)d_origin, &end_rel, cand, s);
+    done_host = st == zfpb::OK || st == zfpb::ERR_TRUNCATED;
+    if (!done_host && st != zfpb::ERR_BAD_INDEX && st != zfpb::ERR_ARGS) return fail(st);
+    if (!done_host) {
+      // Fall back: stage the whole stream for the one-pass path below (which
+      // walks the stream when the index did not match).
+      if (avail && cudaMemcpyAsync(g_stream_stage.p, bs->words + w0, avail * 8, cudaMemcpyHostToDevice, s) !=
+                       cudaSuccess)
+        return fail(zfpb::ERR_CUDA);
+    }
+  }
+  if (!done_host && st != zfpb::ERR_BAD_INDEX)
+    st = zfpb::decompress(call, d_in, avail, start % 64, d_origin, &end_rel, cand, s);
   if (st == zfpb::ERR_BAD_INDEX) {
     // The stream changed since its last compress: stage all of it and walk it.
     bs->index.valid = false;
@@ -1221,7 +1259,7 @@ extern "C" size_t zfp_decompress(zfp_stream* zs, zfp_field* f) {
     st = zfpb::decompress(call, d_in, avail, start % 64, d_origin, &end_rel, nullptr, s);
   }
   if (st != zfpb::OK && st != zfpb::ERR_TRUNCATED) return fail(st);
-  if (host_field &&
+  if (host_field && !done_host &&
       cudaMemcpyAsync(begin, g_field_stage.p, p.span_bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
     return fail(zfpb::ERR_CUDA);
   if (cudaStreamSynchronize(s) != cudaSuccess) return fail(zfpb::ERR_CUDA);

@@ -198,9 +198,9 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const u32* len, u6
 
 // One CTA scans the tile totals in place (exclusive), carrying across rounds,
 // and writes the grand total to *total.
-__global__ void __launch_bounds__(1024) k_scan_partials(u64* partial, u64 m, u64* total) {
+__global__ void __launch_bounds__(1024) k_scan_partials(u64* partial, u64 m, u64* total, const u64* carry_in) {
   __shared__ u64 ws[32];
-  u64 carry = 0;
+  u64 carry = carry_in ? *carry_in : 0;
   for (u64 base = 0; base < m; base += blockDim.x) {
     u64 i = base + threadIdx.x;
     u64 v = i < m ? partial[i] : 0;
@@ -404,12 +404,14 @@ template <class Fn> static cudaError_t for_type(int type, Fn fn) {
   } while (0)
 
 // Exclusive scan of n lengths into off[0..n] (off[n] = total); `part` holds
-// ceil(n / SCAN_TILE) + 1 words.
-static cudaError_t scan_entries(const u32* d_len, u64 n, u64* d_off, u64* part, cudaStream_t s) {
+// ceil(n / SCAN_TILE) + 1 words.  With carry_in (device, read before off is
+// written; it may be off[0] itself) every offset is raised by *carry_in.
+static cudaError_t scan_entries(const u32* d_len, u64 n, u64* d_off, u64* part, cudaStream_t s,
+                                const u64* carry_in = nullptr) {
   u64 tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
   KernelTimer t(K_SCAN, s);
   k_scan_reduce<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(d_len, n, part);
-  k_scan_partials<<<1, 1024, 0, s>>>(part, tiles, d_off + n);
+  k_scan_partials<<<1, 1024, 0, s>>>(part, tiles, d_off + n, carry_in);
   k_scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(d_len, n, part, d_off);
   return cudaGetLastError();
 }
@@ -655,6 +657,295 @@ Status decompress(const Call& call, const u64* d_in, u64 len, u64 start, void* d
   ZFPB_CHECK(cudaStreamSynchronize(s));
   *end_bit = start + ws.h_pinned[1];
   if (fl & FLAG_BAD_INDEX) return ERR_CUDA;
+  return (fl & FLAG_TRUNCATED) ? ERR_TRUNCATED : OK;
+}
+
+// ---------------------------------------------------------------------------
+// Host-buffer pipelines (compress_host / decompress_host).
+//
+// A field with natural strides is cut along its slowest axis into chunks of
+// whole block layers (contiguous in memory and in block order).  Three streams
+// overlap the host->device copy of chunk k+1, the coding of chunk k and the
+// device->host copy of chunk k-1's output, so a call takes about as long as
+// the larger of its two PCIe transfers instead of their sum.
+// ---------------------------------------------------------------------------
+
+// Every word in [wa, wb) assembled from the block slots: each thread finds
+// the block holding its word's first bit (binary search over the offsets)
+// and gathers from there, like k_pack.
+__global__ void __launch_bounds__(256) k_pack_range(PackArgs a, u64 wa, u64 wb) {
+  const u64 w = wa + (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= wb) return;
+  u64 v = 0;
+  u32 fill = 0;
+  u64 pos = w << 6;
+  if (w == (a.start >> 6)) {
+    v = a.init_word;
+    fill = (u32)(a.start & 63);
+    pos = a.start;
+  }
+  const u64 rel = pos - a.start;
+  u64 lo = 0, hi = a.nblocks;  // largest j with off[j] <= rel
+  while (hi - lo > 1) {
+    const u64 mid = (lo + hi) >> 1;
+    if (a.off[mid] <= rel) lo = mid;
+    else hi = mid;
+  }
+  u64 blk = lo;
+  u64 pj = a.start + a.off[blk], qj = a.start + a.off[blk + 1];
+  while (fill < 64 && blk < a.nblocks) {
+    const u64 local = pos - pj;
+    const u64 avail = qj - pos;
+    const u32 take = (u32)(avail < (u64)(64 - fill) ? avail : (u64)(64 - fill));
+    v |= slot_bits(a.slots + blk * a.slot_words, local, take) << fill;
+    fill += take;
+    pos += take;
+    if (pos == qj) {
+      blk++;
+      if (blk < a.nblocks) {
+        pj = qj;
+        qj = a.start + a.off[blk + 1];
+      }
+    }
+  }
+  a.out[w] = v;
+}
+
+namespace {
+
+struct Pipe {
+  cudaStream_t in = nullptr, out = nullptr;
+  std::vector<cudaEvent_t> ev;
+  u64* h_words = nullptr;  // pinned scratch for chunk boundaries
+  u64 h_cap = 0;
+  cudaEvent_t event(size_t i) {
+    while (ev.size() <= i) {
+      cudaEvent_t e;
+      cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+      ev.push_back(e);
+    }
+    return ev[i];
+  }
+  bool pinned(u64 n) {
+    if (n <= h_cap) return true;
+    if (h_words) cudaFreeHost(h_words);
+    h_words = nullptr;
+    h_cap = 0;
+    if (cudaMallocHost((void**)&h_words, n * sizeof(u64)) != cudaSuccess) return false;
+    h_cap = n;
+    return true;
+  }
+};
+Pipe g_pipe;
+
+bool pipe_streams() {
+  if (!g_pipe.in && cudaStreamCreateWithFlags(&g_pipe.in, cudaStreamNonBlocking) != cudaSuccess) return false;
+  if (!g_pipe.out && cudaStreamCreateWithFlags(&g_pipe.out, cudaStreamNonBlocking) != cudaSuccess) return false;
+  return true;
+}
+
+// Chunking of a natural-stride field along its slowest axis.
+struct Layers {
+  int axis;
+  u64 per_layer;   // blocks per block layer
+  u64 layers;      // block layers
+  u64 per_chunk;   // layers per chunk
+  u64 layer_elems; // elements per full block layer (4 rows)
+};
+
+Layers layers_of(const Call& c, u64 es) {
+  Layers L;
+  L.axis = c.dims - 1;
+  L.layers = c.f.b[L.axis];
+  L.per_layer = c.f.nblocks / L.layers;
+  L.layer_elems = 4 * (u64)c.f.s[L.axis];
+  const u64 layer_bytes = L.layer_elems * es;
+  L.per_chunk = std::max<u64>(1, (64ull << 20) / std::max<u64>(1, layer_bytes));
+  return L;
+}
+
+// The sub-field of layers [j0, j1).
+Call sub_call(const Call& c, const Layers& L, u64 j0, u64 j1) {
+  Call s = c;
+  const int a = L.axis;
+  const u64 rows = std::min<u64>(c.f.n[a], 4 * j1) - 4 * j0;
+  s.f.n[a] = rows;
+  s.f.b[a] = j1 - j0;
+  s.f.nblocks = L.per_layer * (j1 - j0);
+  return s;
+}
+
+}  // namespace
+
+bool natural_strides(const Call& c) {
+  i64 want = 1;
+  for (int d = 0; d < c.dims; d++) {
+    if (c.f.s[d] != want) return false;
+    want *= (i64)c.f.n[d];
+  }
+  return true;
+}
+
+Status compress_host(const Call& call, const void* h_field, void* d_field, u64* h_out, u64* d_out, u64 cap,
+                     u64 start, u64 init_word, u64* end_bit, u64* d_offsets, cudaStream_t s) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  Workspace& ws = workspace();
+  const u64 n = call.f.nblocks;
+  const u64 es = (call.type == 1 || call.type == 3) ? 4 : 8;
+  if (n == 0 || !natural_strides(call) || !pipe_streams()) return ERR_ARGS;
+  const Layers L = layers_of(call, es);
+  const u64 nchunks = (L.layers + L.per_chunk - 1) / L.per_chunk;
+  const u64 bb = block_bits(call.c, call.type, call.dims);
+  const u64 slot_words = (bb + 63) / 64 + 1;
+  ZFPB_CHECK(ws.slots.ensure((n * slot_words + 1) * sizeof(u64)));
+  ZFPB_CHECK(ws.lengths.ensure(n * sizeof(u32)));
+  u64* off = d_offsets;
+  if (!off) {
+    ZFPB_CHECK(ws.offsets.ensure((n + 1) * sizeof(u64)));
+    off = (u64*)ws.offsets.p;
+  }
+  const u64 chunk_blocks = L.per_chunk * L.per_layer;
+  ZFPB_CHECK(ws.partial.ensure(((chunk_blocks + SCAN_TILE - 1) / SCAN_TILE + 1) * sizeof(u64)));
+  if (!g_pipe.pinned(nchunks)) return ERR_CUDA;
+  // The first block starts at offset 0 (the carry of chunk 0).
+  ZFPB_CHECK(cudaMemsetAsync(off, 0, sizeof(u64), s));
+  u64 wdone = start >> 6;  // stream words already assembled and copied out
+  const u64 total_words_cap = cap;
+  Status result = OK;
+  auto pack_upto = [&](u64 k, bool last) -> cudaError_t {
+    cudaEventSynchronize(g_pipe.event(3 * k + 1));
+    const u64 end = start + g_pipe.h_words[k];
+    u64 wend = last ? (end + 63) / 64 : end / 64;
+    if ((end + 63) / 64 > total_words_cap) {
+      result = ERR_OVERFLOW;
+      return cudaSuccess;
+    }
+    if (wend <= wdone) return cudaSuccess;
+    PackArgs pa;
+    pa.slots = (u64*)ws.slots.p;
+    pa.slot_words = slot_words;
+    pa.off = off;
+    pa.nblocks = std::min<u64>(n, (k + 1) * chunk_blocks);
+    pa.start = start;
+    pa.init_word = init_word;
+    pa.out = d_out;
+    {
+      KernelTimer t(K_PACK, s);
+      k_pack_range<<<(unsigned)((wend - wdone + 255) / 256), 256, 0, s>>>(pa, wdone, wend);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    cudaEvent_t ep = g_pipe.event(3 * k + 2);
+    cudaEventRecord(ep, s);
+    cudaStreamWaitEvent(g_pipe.out, ep, 0);
+    e = cudaMemcpyAsync(h_out + wdone, d_out + wdone, (wend - wdone) * 8, cudaMemcpyDeviceToHost, g_pipe.out);
+    wdone = wend;
+    return e;
+  };
+  for (u64 k = 0; k < nchunks && result == OK; k++) {
+    const u64 j0 = k * L.per_chunk, j1 = std::min(L.layers, j0 + L.per_chunk);
+    const u64 e0 = j0 * L.layer_elems;
+    const u64 rows = std::min<u64>(call.f.n[L.axis], 4 * j1) - 4 * j0;
+    const u64 bytes = rows * (u64)call.f.s[L.axis] * es;
+    ZFPB_CHECK(cudaMemcpyAsync((char*)d_field + e0 * es, (const char*)h_field + e0 * es, bytes,
+                               cudaMemcpyHostToDevice, g_pipe.in));
+    cudaEvent_t ei = g_pipe.event(3 * k);
+    ZFPB_CHECK(cudaEventRecord(ei, g_pipe.in));
+    ZFPB_CHECK(cudaStreamWaitEvent(s, ei, 0));
+    const Call sub = sub_call(call, L, j0, j1);
+    const u64 b0 = j0 * L.per_layer;
+    EncodeVarArgs ea;
+    ea.data = (const char*)d_field + e0 * es;
+    ea.f = sub.f;
+    ea.c = call.c;
+    ea.slots = (u64*)ws.slots.p + b0 * slot_words;
+    ea.slot_words = slot_words;
+    ea.lengths = (u32*)ws.lengths.p + b0;
+    {
+      KernelTimer t(K_ENCODE_VAR, s);
+      ZFPB_CHECK(for_type(call.type, [&](auto* tp) {
+        using T = std::remove_pointer_t<decltype(tp)>;
+        return Launch<T>::encode_var(sub, ea, s);
+      }));
+    }
+    ZFPB_CHECK(scan_entries((u32*)ws.lengths.p + b0, sub.f.nblocks, off + b0, (u64*)ws.partial.p, s, off + b0));
+    ZFPB_CHECK(cudaMemcpyAsync(g_pipe.h_words + k, off + b0 + sub.f.nblocks, sizeof(u64), cudaMemcpyDeviceToHost, s));
+    ZFPB_CHECK(cudaEventRecord(g_pipe.event(3 * k + 1), s));
+    if (k > 0) ZFPB_CHECK(pack_upto(k - 1, false));
+  }
+  if (result == OK) ZFPB_CHECK(pack_upto(nchunks - 1, true));
+  ZFPB_CHECK(cudaStreamSynchronize(s));
+  ZFPB_CHECK(cudaStreamSynchronize(g_pipe.out));
+  ZFPB_CHECK(cudaStreamSynchronize(g_pipe.in));
+  if (result != OK) return result;
+  *end_bit = start + g_pipe.h_words[nchunks - 1];
+  return OK;
+}
+
+Status decompress_host(const Call& call, const u64* h_in, u64* d_in, u64 len, u64 start, void* h_field,
+                       void* d_field, u64* end_bit, const u64* d_offsets, cudaStream_t s) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  Workspace& ws = workspace();
+  const u64 n = call.f.nblocks;
+  const u64 es = (call.type == 1 || call.type == 3) ? 4 : 8;
+  const bool fixed = fixed_size_blocks(call);
+  if (n == 0 || !natural_strides(call) || (!fixed && !d_offsets) || !pipe_streams()) return ERR_ARGS;
+  const Layers L = layers_of(call, es);
+  const u64 nchunks = (L.layers + L.per_chunk - 1) / L.per_chunk;
+  const u64 chunk_blocks = L.per_chunk * L.per_layer;
+  if (!g_pipe.pinned(nchunks + 1)) return ERR_CUDA;
+  // Chunk boundaries in the stream.
+  for (u64 k = 0; k <= nchunks; k++) {
+    const u64 b = std::min(n, k * chunk_blocks);
+    if (fixed) g_pipe.h_words[k] = b * (u64)call.c.maxbits;
+    else ZFPB_CHECK(cudaMemcpyAsync(g_pipe.h_words + k, d_offsets + b, sizeof(u64), cudaMemcpyDeviceToHost, s));
+  }
+  ZFPB_CHECK(ws.small.ensure(64));
+  unsigned* flags = (unsigned*)ws.small.p;
+  ZFPB_CHECK(cudaMemsetAsync(flags, 0, sizeof(unsigned), s));
+  ZFPB_CHECK(cudaStreamSynchronize(s));
+  u64 wcopied = 0;
+  for (u64 k = 0; k < nchunks; k++) {
+    const u64 j0 = k * L.per_chunk, j1 = std::min(L.layers, j0 + L.per_chunk);
+    const u64 e0 = j0 * L.layer_elems;
+    // Stream words of the chunk's blocks, and two more (the readers look ahead).
+    u64 wb = std::min(len, (start + g_pipe.h_words[k + 1] + 63) / 64 + 2);
+    if (wb > wcopied)
+      ZFPB_CHECK(cudaMemcpyAsync(d_in + wcopied, h_in + wcopied, (wb - wcopied) * 8, cudaMemcpyHostToDevice,
+                                 g_pipe.in));
+    wcopied = std::max(wcopied, wb);
+    cudaEvent_t ei = g_pipe.event(3 * k);
+    ZFPB_CHECK(cudaEventRecord(ei, g_pipe.in));
+    ZFPB_CHECK(cudaStreamWaitEvent(s, ei, 0));
+    const Call sub = sub_call(call, L, j0, j1);
+    const u64 b0 = j0 * L.per_layer;
+    DecodeArgs a;
+    a.data = (char*)d_field + e0 * es;
+    a.f = sub.f;
+    a.c = call.c;
+    a.stream = d_in;
+    a.stream_len = len;
+    a.start = fixed ? start + b0 * (u64)call.c.maxbits : start;
+    a.offsets = fixed ? nullptr : const_cast<u64*>(d_offsets) + b0;
+    a.flags = flags;
+    a.owner = nullptr;
+    a.imin = 0;
+    ZFPB_CHECK(decode_blocks(ws, sub, a, !fixed, s));
+    cudaEvent_t ed = g_pipe.event(3 * k + 1);
+    ZFPB_CHECK(cudaEventRecord(ed, s));
+    ZFPB_CHECK(cudaStreamWaitEvent(g_pipe.out, ed, 0));
+    const u64 rows = std::min<u64>(call.f.n[L.axis], 4 * j1) - 4 * j0;
+    const u64 bytes = rows * (u64)call.f.s[L.axis] * es;
+    ZFPB_CHECK(cudaMemcpyAsync((char*)h_field + e0 * es, (char*)d_field + e0 * es, bytes, cudaMemcpyDeviceToHost,
+                               g_pipe.out));
+  }
+  ZFPB_CHECK(cudaMemcpyAsync(ws.h_pinned, flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  ZFPB_CHECK(cudaStreamSynchronize(s));
+  ZFPB_CHECK(cudaStreamSynchronize(g_pipe.out));
+  ZFPB_CHECK(cudaStreamSynchronize(g_pipe.in));
+  const unsigned fl = *(unsigned*)ws.h_pinned;
+  *end_bit = start + g_pipe.h_words[nchunks];
+  if (fl & FLAG_BAD_INDEX) return ERR_BAD_INDEX;
   return (fl & FLAG_TRUNCATED) ? ERR_TRUNCATED : OK;
 }
 
@@ -1397,7 +1688,7 @@ Status compress_noalloc(const Call& call, const void* d_field, u64* d_out, u64 c
     return Launch<T>::encode_var(call, ea, s);
   }));
   k_scan_reduce<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(lengths, n, part);
-  k_scan_partials<<<1, 1024, 0, s>>>(part, tiles, off + n);
+  k_scan_partials<<<1, 1024, 0, s>>>(part, tiles, off + n, nullptr);
   k_scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(lengths, n, part, off);
   ZFPB_CHECK(cudaGetLastError());
   u64 total = 0;

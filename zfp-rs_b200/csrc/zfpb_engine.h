@@ -113,6 +113,19 @@ Status compress(const Call& call, const void* d_field, u64* d_out, u64 cap, u64 
 Status decompress(const Call& call, const u64* d_in, u64 len, u64 start, void* d_field, u64* end_bit,
                   const u64* d_offsets, cudaStream_t s);
 
+// Host buffers, copies overlapped with coding (fields with natural strides).
+// compress_host: h_field is the host field (element [0,0,0,0]), d_field a
+// device buffer of the same size; the stream goes to the host words h_out
+// (cap words) through d_out, from bit `start` (< 64) whose word holds
+// init_word.  decompress_host: h_in / d_in (len words) hold / receive the
+// stream; block offsets are needed unless blocks are fixed-size.  Both return
+// ERR_ARGS when the field does not qualify (then use compress / decompress).
+bool natural_strides(const Call& call);
+Status compress_host(const Call& call, const void* h_field, void* d_field, u64* h_out, u64* d_out, u64 cap,
+                     u64 start, u64 init_word, u64* end_bit, u64* d_offsets, cudaStream_t s);
+Status decompress_host(const Call& call, const u64* h_in, u64* d_in, u64 len, u64 start, void* h_field,
+                       void* d_field, u64* end_bit, const u64* d_offsets, cudaStream_t s);
+
 // ---- batches ---------------------------------------------------------------
 //
 // A batch codes many arrays of mixed type, dimensionality, size and mode in a
