@@ -1167,7 +1167,86 @@ struct Window {
     }
   }
   ZFPB_DEV u64 pos() const { return ((next - 3) << 6) + off; }
+  // Any distance: re-reads the three words at the new position.
+  ZFPB_DEV void advance_far(u64 n) {
+    const u64 p = pos() + n;
+    init(rd, p);
+  }
 };
+
+// One plane's group-test code, from bit 0 of the 128-bit window (t0, t1)
+// whose bit 0 is a 1 (at least one new significant coefficient), with n
+// coefficients significant before the plane and a bits of budget left for
+// the code.  Sets end (the code's length), n_new and m_new (n and m of the
+// reference's reader after the plane) and, with NEED_Y, y: the plane's bits
+// from coefficient n up, as the reader would set them.
+template <int N, bool NEED_Y>
+ZFPB_DEV void group_tests(u64 t0, u64 t1, u32 n, u32 a, u32& end, u32& n_new, u32& m_new, u64& y) {
+  constexpr u32 size = N;
+  constexpr bool WIDE = N == 64;
+  const u64 p0 = prefix_xor64(t0);
+  const u64 p1 = WIDE ? prefix_xor64(t1) ^ (0ull - (p0 >> 63)) : 0ull;
+  const u64 s0 = t0 & ~p0, s1 = t1 & ~p1;  // coefficient ones
+  const u64 g0 = t0 & p0, g1 = t1 & p1;    // GT ones
+  const u64 b0 = (s0 << 1) | 1, b1 = (s1 << 1) | (s0 >> 63);  // group starts
+  const u32 e = WIDE ? (((b0 & ~t0) != 0) ? ctz64(b0 & ~t0) : 64 + ctz64(b1 & ~t1)) : ctz64(b0 & ~t0);
+  const u32 lim = WIDE ? 128 : 64;
+  const u32 ce = n + e - popc_below128(g0, g1, e);  // coefficients read before bit e
+  const bool regular = e < lim && ce <= size - 1;
+  u32 extra = 64;
+  if (regular && e < a) {
+    end = e + 1;
+    n_new = ce;
+    m_new = size;
+  } else {
+    // Ended by the implied last one (not a terminator), or cut by the budget.
+    u32 istar = lim;
+    u32 bs = 0;
+    if (!regular) {
+      const u32 L = size - 1 - n;  // coefficient zeros before the implied one
+      istar = L == 0 ? 0 : select128(~g0, WIDE ? ~g1 : 0ull, L - 1) + 1;
+      bs = bit128(b0, b1, istar < lim ? istar : 0);
+    }
+    if (!regular && (bs ? istar < a : istar <= a)) {
+      end = istar + bs;
+      extra = size - 1 - n;
+      n_new = size;
+      m_new = size;
+    } else {
+      end = a;  // a < lim here
+      const u32 ca = n + a - popc_below128(g0, g1, a);
+      if (bit128(b0, b1, a)) {
+        n_new = ca;
+      } else {
+        extra = ca - n;  // the reader's implied one at the cut
+        n_new = ca + 1;
+      }
+      m_new = n_new;
+    }
+  }
+  if constexpr (!NEED_Y) {
+    y = 0;
+    return;
+  }
+  // Coefficient ones before `end`, each moved down past the GT bits
+  // before it: the j-th (from 1) at bit s goes to coefficient s - j.
+  u64 q0 = s0 & low_mask(end < 64 ? end : 64);
+  u64 q1 = (WIDE && end > 64) ? s1 & low_mask(end - 64) : 0ull;
+  y = extra < 64 ? 1ull << extra : 0ull;
+  u32 j = 1;
+  while (q0) {
+    y |= 1ull << (ctz64(q0) - j);
+    j++;
+    q0 &= q0 - 1;
+  }
+  if (WIDE) {
+    while (q1) {
+      y |= 1ull << (64 + ctz64(q1) - j);
+      j++;
+      q1 &= q1 - 1;
+    }
+  }
+}
 
 // Same contract and results as decode_planes, for N <= 64.
 template <int N>
@@ -1240,65 +1319,9 @@ ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 in
           bits -= 1;
           m = size;
         } else {
-          const u64 p0 = prefix_xor64(t0);
-          const u64 p1 = WIDE ? prefix_xor64(t1) ^ (0ull - (p0 >> 63)) : 0ull;
-          const u64 s0 = t0 & ~p0, s1 = t1 & ~p1;  // coefficient ones
-          const u64 g0 = t0 & p0, g1 = t1 & p1;    // GT ones
-          const u64 b0 = (s0 << 1) | 1, b1 = (s1 << 1) | (s0 >> 63);  // group starts
-          const u32 e = WIDE ? (((b0 & ~t0) != 0) ? ctz64(b0 & ~t0) : 64 + ctz64(b1 & ~t1)) : ctz64(b0 & ~t0);
-          const u32 lim = WIDE ? 128 : 64;
-          const u32 ce = n + e - popc_below128(g0, g1, e);  // coefficients read before bit e
-          const bool regular = e < lim && ce <= size - 1;
-          const u32 a = bits;  // budget left for the code
-          u32 end, extra = 64, n_new, m_new;
-          if (regular && e < a) {
-            end = e + 1;
-            n_new = ce;
-            m_new = size;
-          } else {
-            // Ended by the implied last one (not a terminator), or cut by the budget.
-            u32 istar = lim;
-            u32 bs = 0;
-            if (!regular) {
-              const u32 L = size - 1 - n;  // coefficient zeros before the implied one
-              istar = L == 0 ? 0 : select128(~g0, WIDE ? ~g1 : 0ull, L - 1) + 1;
-              bs = bit128(b0, b1, istar < lim ? istar : 0);
-            }
-            if (!regular && (bs ? istar < a : istar <= a)) {
-              end = istar + bs;
-              extra = size - 1 - n;
-              n_new = size;
-              m_new = size;
-            } else {
-              end = a;  // a < lim here
-              const u32 ca = n + a - popc_below128(g0, g1, a);
-              if (bit128(b0, b1, a)) {
-                n_new = ca;
-              } else {
-                extra = ca - n;  // the reader's implied one at the cut
-                n_new = ca + 1;
-              }
-              m_new = n_new;
-            }
-          }
-          // Coefficient ones before `end`, each moved down past the GT bits
-          // before it: the j-th (from 1) at bit s goes to coefficient s - j.
-          u64 q0 = s0 & low_mask(end < 64 ? end : 64);
-          u64 q1 = (WIDE && end > 64) ? s1 & low_mask(end - 64) : 0ull;
-          u64 y = extra < 64 ? 1ull << extra : 0ull;
-          u32 j = 1;
-          while (q0) {
-            y |= 1ull << (ctz64(q0) - j);
-            j++;
-            q0 &= q0 - 1;
-          }
-          if (WIDE) {
-            while (q1) {
-              y |= 1ull << (64 + ctz64(q1) - j);
-              j++;
-              q1 &= q1 - 1;
-            }
-          }
+          u32 end, n_new, m_new;
+          u64 y;
+          group_tests<N, true>(t0, t1, n, bits, end, n_new, m_new, y);
           x |= y << n;
           used += end;
           bits -= end;
@@ -1611,6 +1634,125 @@ ZFPB_DEV u32 decode_block(Reader& r, T* blk, const Codec& c, PlaneStore ps, u32*
   } else {
     bits = decode_int_block<I, N>(r, c.maxbits, c.maxprec, c.rounding, blk, ps);
     *read_bits = bits;
+    return bits < c.minbits ? c.minbits : bits;
+  }
+}
+
+// Bits of the planes of one block, as decode_planes_sync reads them, without
+// the planes: group-test planes one at a time, and once every coefficient is
+// significant the verbatim planes left all at once (min(bits, planes * size)).
+// For the offsets of streams that come without an index.
+template <int N>
+ZFPB_DEV u32 plane_bits(Reader& rd, u32 budget, u32 kmin, u32 intprec) {
+  static_assert(N <= 64, "one plane word per plane");
+  constexpr u32 size = N;
+  constexpr bool WIDE = N == 64;
+  Window r;
+  r.init(&rd, rd.pos());
+  u32 bits = budget, n = 0, k = intprec;
+  while (bits != 0 && k > kmin) {
+    if (n == size) {
+      const u64 rest = (u64)(k - kmin) * size;
+      const u32 take = rest < bits ? (u32)rest : bits;
+      r.advance_far(take);
+      bits -= take;
+      break;
+    }
+    const u64 lo = r.lo();
+    if (n == 0) {
+      u32 e = ctz64(lo);
+      e = e < k - kmin ? e : k - kmin;
+      e = e < bits ? e : bits;
+      if (e != 0) {
+        r.advance(e);
+        bits -= e;
+        k -= e;
+        continue;
+      }
+    }
+    k--;
+    if constexpr (N == 4) {
+      const u32 e = kPlane4.dec[n * 256 + (u32)(lo & 0xff)];
+      const u32 len = (e >> 4) & 15u;
+      if (len != 0 && len <= bits) {
+        n = e >> 8;
+        bits -= len;
+        r.advance(len);
+        continue;
+      }
+    }
+    u32 used = n < bits ? n : bits;
+    bits -= used;
+    if (bits != 0) {
+      const u64 hi = WIDE ? r.hi() : 0ull;
+      const u64 t0 = n ? (lo >> n) | (hi << (64 - n)) : lo;
+      const u64 t1 = n ? hi >> n : hi;
+      if ((t0 & 1) == 0) {
+        used += 1;
+        bits -= 1;
+      } else {
+        u32 end, n_new, m_new;
+        u64 y;
+        group_tests<N, false>(t0, t1, n, bits, end, n_new, m_new, y);
+        used += end;
+        bits -= end;
+        n = n_new;
+      }
+    }
+    r.advance(used);
+  }
+  rd.init(rd.src, rd.len, r.pos());
+  return budget - bits;
+}
+
+// decode_ints' bits without the planes.
+template <class U, int N>
+ZFPB_DEV u32 ints_bits(Reader& r, u32 maxbits, u32 maxprec) {
+  constexpr u32 intprec = sizeof(U) * 8;
+  const bool constrained = with_maxbits(maxbits, maxprec, N);
+  const u32 kmin = intprec > maxprec ? intprec - maxprec : 0;
+  return plane_bits<N>(r, constrained ? maxbits : 0xffffffffu, kmin, intprec);
+}
+
+// The bits one block occupies (after the skip to minbits), read as
+// decode_block reads them (same headers), without decoding its values.
+template <class T, int N>
+ZFPB_DEV u32 block_length(Reader& r, const Codec& c) {
+  typedef typename Traits<T>::U U;
+  constexpr u32 PB = sizeof(U) == 4 ? 5 : 6;
+  u32 bits;
+  if (c.minexp < ZFP_MIN_EXP) {
+    if constexpr (!Traits<T>::FLOAT) {
+      const u32 prec = (u32)r.read(PB) + 1;
+      bits = PB + ints_bits<U, N>(r, sat_sub(c.maxbits, PB), prec);
+    } else {
+      if (r.read_bit() == 0) {
+        bits = 1;
+      } else {
+        bits = 2;
+        if (!r.read_bit()) {
+          r.read(Traits<T>::EBITS);
+          bits += Traits<T>::EBITS;
+        }
+        const u32 mb = sat_sub(c.maxbits, bits);
+        const u32 prec = (u32)r.read(PB) + 1;
+        bits += PB + ints_bits<U, N>(r, sat_sub(mb, PB), prec);
+      }
+    }
+    return bits < c.minbits ? c.minbits : bits;
+  }
+  if constexpr (Traits<T>::FLOAT) {
+    if (r.read_bit()) {
+      constexpr u32 hb = 1 + Traits<T>::EBITS;
+      const int emax = (int)r.read(Traits<T>::EBITS) - Traits<T>::EBIAS;
+      const u32 prec = precision_f(emax, c.maxprec, c.minexp, Dims<N>::value, c.tight != 0);
+      const u32 ibits = ints_bits<U, N>(r, sat_sub(c.maxbits, hb), prec);
+      const u32 mb = sat_sub(c.minbits, hb);
+      return hb + (ibits < mb ? mb : ibits);
+    }
+    return c.minbits > 1 ? c.minbits : 1;
+  } else {
+    bits = ints_bits<U, N>(r, c.maxbits, c.maxprec);
     return bits < c.minbits ? c.minbits : bits;
   }
 }

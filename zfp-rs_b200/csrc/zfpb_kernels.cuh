@@ -418,9 +418,13 @@ __global__ void __launch_bounds__(32) k_walk(DecodeArgs a) {
     a.offsets[blk] = rel;
     Reader r;
     r.init(a.stream, a.stream_len, a.start + rel);
-    BlockHead h;
-    u32 rb;
-    rel += parse_block<T, S::N>(r, a.c, ps, h, &rb);
+    if constexpr (S::N <= 64) {
+      rel += block_length<T, S::N>(r, a.c);
+    } else {
+      BlockHead h;
+      u32 rb;
+      rel += parse_block<T, S::N>(r, a.c, ps, h, &rb);
+    }
   }
   a.offsets[a.f.nblocks] = rel;
 }
@@ -568,9 +572,13 @@ __global__ void __launch_bounds__(64) k_walk_batch(BatchArgs a) {
     off[blk] = rel;
     Reader r;
     r.init(it->stream, it->stream_words, rel);
-    BlockHead h;
-    u32 rb;
-    rel += parse_block<T, S::N>(r, c, ps, h, &rb);
+    if constexpr (S::N <= 64) {
+      rel += block_length<T, S::N>(r, c);
+    } else {
+      BlockHead h;
+      u32 rb;
+      rel += parse_block<T, S::N>(r, c, ps, h, &rb);
+    }
   }
   off[n] = rel;
 }
