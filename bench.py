@@ -46,7 +46,7 @@ HBM_FALLBACK_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=512, help="cube side (default 512)")
@@ -124,47 +124,69 @@ def smooth_f32(n, device, seed=0):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clocks and clock-event (throttle) reasons during the timed region,
+    read through NVML every 2 ms from a thread (read-only queries); the
+    samples also go to a CSV file."""
 
-    def __init__(self, index: int, path: Path):
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
+
+    def __init__(self, device_index: int, path: Path):
+        import threading
+
         self.path = path
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.samples = []
+        self.stop_flag = False
         try:
-            self.f = open(path, "w")
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={q}", "--format=csv,noheader",
-                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml as nv
+            import torch
+
+            nv.nvmlInit()
+            h = None
+            uuid = getattr(torch.cuda.get_device_properties(device_index), "uuid", None)
+            if uuid is not None:
+                try:
+                    h = nv.nvmlDeviceGetHandleByUUID(("GPU-" + str(uuid)).encode())
+                except Exception:
+                    h = None
+            if h is None:
+                h = nv.nvmlDeviceGetHandleByIndex(device_index)
+            self.nv, self.h = nv, h
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.get_reasons = get_reasons
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
         except Exception:
-            self.p = None
+            self.nv = None
+
+    def _run(self):
+        nv, h = self.nv, self.h
+        while not self.stop_flag:
+            try:
+                self.samples.append((time.perf_counter(), float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                     int(self.get_reasons(h))))
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def stop(self):
-        if self.p is None:
+        if self.nv is None:
             return None
-        self.p.terminate()
+        self.stop_flag = True
+        self.t.join(timeout=5)
         try:
-            self.p.wait(timeout=5)
+            with open(self.path, "w") as f:
+                f.write("t_s,sm_mhz,reasons_mask\n")
+                for t, mhz, r in self.samples:
+                    f.write(f"{t:.4f},{mhz:.0f},{r:#x}\n")
         except Exception:
-            self.p.kill()
-        self.f.close()
-        sm, mx, reasons = [], [], set()
-        for line in self.path.read_text().splitlines():
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1].split()[0]))
-                mx.append(float(parts[2].split()[0]))
-            except ValueError:
-                continue
-            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-            for name, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(name)
-        if not sm:
+            pass
+        if not self.samples:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = sorted(name for name, bit in self.REASONS.items() if any(r & bit for _, _, r in self.samples))
+        return {"sm_mhz": float(np.median([m for _, m, _ in self.samples])), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples), "source": "NVML, every 2 ms"}
 
 
 def dist_setup(args):
