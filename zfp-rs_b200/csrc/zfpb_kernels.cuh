@@ -214,7 +214,7 @@ template <class T, int D> struct KernelShape {
   // CTAs of 128 threads per SM the register allocation must allow: 4 caps
   // 32-bit blocks at 128 registers (16 warps per SM), 2 caps 64-bit ones at
   // 255.  Occupancy hides the latency of the sequential bit-plane coding.
-  static constexpr int MIN_CTAS = sizeof(T) == 4 ? 4 : 2;
+  static constexpr int MIN_CTAS = sizeof(T) == 4 ? 4 : 3;
 };
 
 // ---------------------------------------------------------------------------
