@@ -484,6 +484,120 @@ template <class U, int N> ZFPB_DEV void load_planes(U* u, PlaneStore ps, int lo,
   }
 }
 
+// ---- register planes of 4-value blocks ------------------------------------
+//
+// A 1D block's P = bits-of-U planes are 4 bits each, so all of them fit in
+// P / 16 registers as a nibble string: plane k is nibble P - 1 - k (bit i of
+// the nibble is bit k of u[i]).  Planes are coded from the top down, so a run
+// of planes is a contiguous run of nibbles, in the order the stream carries a
+// verbatim run.  Word w of the string holds nibbles 16w .. 16w + 15.
+
+// Swaps bits a and a + D of x for every position a in the mask.
+template <int D> ZFPB_DEV u64 delta_swap(u64 x, u64 mask) {
+  const u64 t = ((x >> D) ^ x) & mask;
+  return x ^ t ^ (t << D);
+}
+
+// Nibble-major (bit 4j + i) to lane-major (bit 16i + j): the 6 index bits
+// [j3 j2 j1 j0 i1 i0] rotate to [i1 i0 j3 j2 j1 j0], as two 3-cycles of index
+// bits, each two transpositions (index bits p < q swap with D = 2^q - 2^p on
+// the positions whose bit p is 1 and bit q is 0).
+ZFPB_DEV u64 nibbles_to_lanes(u64 x) {
+  x = delta_swap<15>(x, 0x0000AAAA0000AAAAull);  // index bits 0, 4
+  x = delta_swap<3>(x, 0x0A0A0A0A0A0A0A0Aull);   // 0, 2
+  x = delta_swap<30>(x, 0x00000000CCCCCCCCull);  // 1, 5
+  x = delta_swap<6>(x, 0x00CC00CC00CC00CCull);   // 1, 3
+  return x;
+}
+
+ZFPB_DEV u64 lanes_to_nibbles(u64 x) {
+  x = delta_swap<6>(x, 0x00CC00CC00CC00CCull);
+  x = delta_swap<30>(x, 0x00000000CCCCCCCCull);
+  x = delta_swap<3>(x, 0x0A0A0A0A0A0A0A0Aull);
+  x = delta_swap<15>(x, 0x0000AAAA0000AAAAull);
+  return x;
+}
+
+ZFPB_DEV u32 rev32(u32 x) {
+#ifdef __CUDA_ARCH__
+  return __brev(x);
+#else
+  x = ((x >> 1) & 0x55555555u) | ((x & 0x55555555u) << 1);
+  x = ((x >> 2) & 0x33333333u) | ((x & 0x33333333u) << 2);
+  x = ((x >> 4) & 0x0F0F0F0Fu) | ((x & 0x0F0F0F0Fu) << 4);
+  x = ((x >> 8) & 0x00FF00FFu) | ((x & 0x00FF00FFu) << 8);
+  return (x >> 16) | (x << 16);
+#endif
+}
+
+// Low 16 bits of a, then low 16 bits of b (LO) or the high halves (HI).
+ZFPB_DEV u32 pair_lo16(u32 a, u32 b) { return (a & 0xffffu) | (b << 16); }
+ZFPB_DEV u32 pair_hi16(u32 a, u32 b) { return (a >> 16) | (b & 0xffff0000u); }
+
+// u[0..3] -> the nibble string q[0 .. P/16).
+template <class U> ZFPB_DEV void store_nibbles(const U* u, u64* q) {
+  if constexpr (sizeof(U) == 4) {
+    // t_i = reversed u[i]: bit m of t_i is bit i of nibble m.
+    const u32 t0 = rev32(u[0]), t1 = rev32(u[1]), t2 = rev32(u[2]), t3 = rev32(u[3]);
+    q[0] = lanes_to_nibbles((u64)pair_lo16(t0, t1) | ((u64)pair_lo16(t2, t3) << 32));
+    q[1] = lanes_to_nibbles((u64)pair_hi16(t0, t1) | ((u64)pair_hi16(t2, t3) << 32));
+  } else {
+    u32 lo[4], hi[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      lo[i] = rev32((u32)((u64)u[i] >> 32));  // nibbles 0..31 come from the high half
+      hi[i] = rev32((u32)u[i]);
+    }
+    q[0] = lanes_to_nibbles((u64)pair_lo16(lo[0], lo[1]) | ((u64)pair_lo16(lo[2], lo[3]) << 32));
+    q[1] = lanes_to_nibbles((u64)pair_hi16(lo[0], lo[1]) | ((u64)pair_hi16(lo[2], lo[3]) << 32));
+    q[2] = lanes_to_nibbles((u64)pair_lo16(hi[0], hi[1]) | ((u64)pair_lo16(hi[2], hi[3]) << 32));
+    q[3] = lanes_to_nibbles((u64)pair_hi16(hi[0], hi[1]) | ((u64)pair_hi16(hi[2], hi[3]) << 32));
+  }
+}
+
+// The nibble string q -> u[0..3].
+template <class U> ZFPB_DEV void load_nibbles(U* u, const u64* q) {
+  if constexpr (sizeof(U) == 4) {
+    const u64 a = nibbles_to_lanes(q[0]), b = nibbles_to_lanes(q[1]);
+    u[0] = rev32(pair_lo16((u32)a, (u32)b));
+    u[1] = rev32(pair_hi16((u32)a, (u32)b));
+    u[2] = rev32(pair_lo16((u32)(a >> 32), (u32)(b >> 32)));
+    u[3] = rev32(pair_hi16((u32)(a >> 32), (u32)(b >> 32)));
+  } else {
+    const u64 a = nibbles_to_lanes(q[0]), b = nibbles_to_lanes(q[1]);
+    const u64 c = nibbles_to_lanes(q[2]), d = nibbles_to_lanes(q[3]);
+    u[0] = ((u64)rev32(pair_lo16((u32)a, (u32)b)) << 32) | rev32(pair_lo16((u32)c, (u32)d));
+    u[1] = ((u64)rev32(pair_hi16((u32)a, (u32)b)) << 32) | rev32(pair_hi16((u32)c, (u32)d));
+    u[2] = ((u64)rev32(pair_lo16((u32)(a >> 32), (u32)(b >> 32))) << 32) |
+           rev32(pair_lo16((u32)(c >> 32), (u32)(d >> 32)));
+    u[3] = ((u64)rev32(pair_hi16((u32)(a >> 32), (u32)(b >> 32))) << 32) |
+           rev32(pair_hi16((u32)(c >> 32), (u32)(d >> 32)));
+  }
+}
+
+// The 64 bits of the nibble string from bit `pos` (zeros past its end).
+template <int W> ZFPB_DEV u64 nibbles_at(const u64* q, u32 pos) {
+  const u32 wi = pos >> 6, s = pos & 63;
+  u64 a = 0, b = 0;
+#pragma unroll
+  for (int w = 0; w < W; w++) {
+    if ((u32)w == wi) a = q[w];
+    if ((u32)w == wi + 1) b = q[w];
+  }
+  return s ? (a >> s) | (b << (64 - s)) : a;
+}
+
+// OR x into the nibble string from bit `pos` (bits past its end dropped).
+template <int W> ZFPB_DEV void nibbles_or(u64* q, u32 pos, u64 x) {
+  const u32 wi = pos >> 6, s = pos & 63;
+  const u64 a = x << s, b = s ? x >> (64 - s) : 0ull;
+#pragma unroll
+  for (int w = 0; w < W; w++) {
+    if ((u32)w == wi) q[w] |= a;
+    if ((u32)w == wi + 1) q[w] |= b;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Bit I/O.  Streams are 64-bit words, bits least-significant first
 // (zfp-rs src/bitstream/core.rs).
@@ -873,7 +987,10 @@ ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore
     u32 top;
     if constexpr (sizeof(U) == 4) top = 32 - __clz((int)all);
     else top = 64 - __clzll((long long)all);
-    store_planes<U, N>(u, ps);
+    constexpr int QW = N == 4 ? (int)intprec / 16 : 1;
+    u64 q[QW];
+    if constexpr (N == 4) store_nibbles<U>(u, q);
+    else store_planes<U, N>(u, ps);
 
     u32 bits = budget;
     u32 n = 0;
@@ -886,9 +1003,9 @@ ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore
     while (bits != 0 && k > kmin) {
       if (N <= 16 && n == size) break;  // verbatim tail below
       k--;
-      const u64 x = ps.at(k, 0, 1);
       if constexpr (N == 4) {
-        const u32 e = kPlane4.enc[n * 16 + (u32)x];
+        const u32 x = (u32)nibbles_at<QW>(q, 4 * (intprec - 1 - k)) & 15u;
+        const u32 e = kPlane4.enc[n * 16 + x];
         const u32 len = (e >> 8) & 15u;
         const u32 take = len < bits ? len : bits;
         w.put(e & low_mask(take), take);
@@ -896,6 +1013,7 @@ ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore
         n = e >> 12;
         continue;
       }
+      const u64 x = ps.at(k, 0, 1);
       if (n == size) {
         const u32 take = size < bits ? size : bits;
         w.put(x & low_mask(take), take);
@@ -941,9 +1059,13 @@ ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore
       while (bits != 0 && k > kmin) {
         u64 chunk = 0;
         const u32 np = k - kmin < per ? k - kmin : per;
+        if constexpr (N == 4) {
+          chunk = nibbles_at<QW>(q, 4 * (intprec - k));  // planes k - 1, k - 2, ...
+        } else {
 #pragma unroll
-        for (u32 j = 0; j < per; j++)
-          if (j < np) chunk |= (ps.at(k - 1 - j, 0, 1) & low_mask(size)) << (j * size);
+          for (u32 j = 0; j < per; j++)
+            if (j < np) chunk |= (ps.at(k - 1 - j, 0, 1) & low_mask(size)) << (j * size);
+        }
         const u32 want = np * size;
         const u32 take = want < bits ? want : bits;
         w.put(chunk & low_mask(take), take);
@@ -1248,11 +1370,25 @@ ZFPB_DEV void group_tests(u64 t0, u64 t1, u32 n, u32 a, u32& end, u32& n_new, u3
   }
 }
 
-// Same contract and results as decode_planes, for N <= 64.
-template <int N>
-ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 intprec, PlaneStore ps) {
+// Same contract and results as decode_planes, for N <= 64.  With QW != 0
+// (4-value blocks of QW * 16 planes) the planes go to the nibble string q
+// instead of the plane store.
+template <int N, int QW = 0>
+ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 intprec, PlaneStore ps,
+                                        u64* q = nullptr) {
   static_assert(N <= 64, "one plane word per plane");
+  static_assert(QW == 0 || N == 4, "nibble planes are for 4-value blocks");
   constexpr u32 size = N;
+  // Plane kk (its bits and, with `np` planes, the ones below it) to the store.
+  auto put = [&](u32 kk, u64 x, u32 np) {
+    if constexpr (QW != 0) {
+      nibbles_or<QW>(q, 4 * (QW * 16 - 1 - kk), x);
+    } else {
+#pragma unroll
+      for (u32 j = 0; j < 64 / size; j++)
+        if (j < np) ps.at(kk - j, 0, 1) = (x >> (j * size)) & low_mask(size);
+    }
+  };
   constexpr bool WIDE = N == 64;  // the window needs its second word
   Window r;
   r.init(&rd, rd.pos());
@@ -1286,7 +1422,7 @@ ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 in
       const u32 e = kPlane4.dec[n * 256 + (u32)(lo & 0xff)];
       const u32 len = (e >> 4) & 15u;
       if (len != 0 && len <= bits) {
-        ps.at(k, 0, 1) = e & 15u;
+        put(k, e & 15u, 1);
         if (high < 0) high = (int)k;
         low = (int)k;
         n = e >> 8;
@@ -1331,7 +1467,8 @@ ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 in
       }
     }
     r.advance(used);
-    ps.at(k, 0, 1) = x;
+    if constexpr (N == 4) put(k, x, 1);
+    else ps.at(k, 0, 1) = x;
     if (high < 0) high = (int)k;
     low = (int)k;
   }
@@ -1354,16 +1491,14 @@ ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 in
         u32 np = (bits - 1) / size;
         np = np < per ? np : per;
         np = np < k + 1 - kmin ? np : k + 1 - kmin;
-#pragma unroll
-        for (u32 j = 0; j < per; j++)
-          if (j < np) ps.at(k - j, 0, 1) = (lo >> (j * size)) & low_mask(size);
+        put(k, lo & low_mask(np * size), np);
         if (high < 0) high = (int)k;
         k -= np - 1;
         low = (int)k;
         bits -= np * size;
         r.advance(np * size);
       } else {
-        ps.at(k, 0, 1) = lo & low_mask(bits);
+        put(k, lo & low_mask(bits), 1);
         if (high < 0) high = (int)k;
         low = (int)k;
         m = bits;
@@ -1392,12 +1527,18 @@ ZFPB_DEV u32 decode_ints(Reader& r, u32 maxbits, u32 maxprec, int rounding, U* u
   const u32 budget = constrained ? maxbits : 0xffffffffu;
   const u32 kmin = intprec > maxprec ? intprec - maxprec : 0;
   PlaneResult pr;
-  if constexpr (N <= 64) pr = decode_planes_sync<N>(r, budget, kmin, intprec, ps);
+  constexpr int QW = N == 4 ? (int)intprec / 16 : 0;
+  u64 q[QW ? QW : 1];
+#pragma unroll
+  for (int w = 0; w < (QW ? QW : 1); w++) q[w] = 0;
+  if constexpr (N <= 64) pr = decode_planes_sync<N, QW>(r, budget, kmin, intprec, ps, q);
   else pr = decode_planes<N>(r, budget, kmin, intprec, ps);
   bool z = pr.low == (int)intprec;
   if (z) {
 #pragma unroll
     for (int i = 0; i < N; i++) u[i] = 0;
+  } else if constexpr (QW != 0) {
+    load_nibbles<U>(u, q);
   } else {
     load_planes<U, N>(u, ps, pr.low, pr.high);
   }

@@ -76,6 +76,7 @@ static void index_span(const FieldGeom& f, int dims, i64* imin, i64* imax) {
 }
 
 size_t plane_bytes(int type, int dims) {
+  if (dims == 1) return 0;  // 4-value blocks keep their planes in registers
   size_t prec = (type == 1 || type == 3) ? 32 : 64;
   size_t w = dims == 4 ? 4 : 1;
   return prec * w * sizeof(u64);
@@ -269,20 +270,26 @@ __device__ __forceinline__ u64 slot_bits(const u64* slot, u64 local, u32 take) {
   return take < 64 ? x & ((1ull << take) - 1) : x;
 }
 
-// One warp per 32 consecutive blocks.  The warp's blocks own a contiguous run
+// One warp per BW consecutive blocks.  The warp's blocks own a contiguous run
 // of stream words; lane l assembles words l, l + 32, ... of that run, finding
 // each word's owner among the warp's block offsets (kept in shared memory), so
 // slot reads and stream writes are coalesced and the lanes' loads do not wait
-// on one another.  A word that runs past its owner's end takes the rest of its
-// bits from the blocks after it.  Block i's bits start at delta + off[i]; only
-// words below `cap` are written.
+// on one another.  A word that runs past its owner's end
+// takes the rest of its bits from the blocks after it.  Block i's bits start
+// at delta + off[i]; only words below `cap` are written.  Small blocks (1D,
+// 2D) use more blocks per warp so that a warp has enough words to share out.
+template <int BW>
 __device__ void pack_warp(const u64* slots, u64 slot_words, const u64* off, u64 delta, u64 nblocks, u64 start,
                           u64 init_word, u64* out, u64 cap, u64 b0, u64* po, u32 lane) {
-  const u32 nb = (u32)(nblocks - b0 < 32 ? nblocks - b0 : 32);
+  const u32 nb = (u32)(nblocks - b0 < BW ? nblocks - b0 : BW);
   for (u32 t = lane; t <= nb; t += 32) po[t] = delta + off[b0 + t];
   __syncwarp();
   const u64 wbeg = b0 == 0 ? start >> 6 : (po[0] + 63) >> 6;
   const u64 wend = (po[nb] + 63) >> 6;
+  // Blocks of 8 words or more on average: the owner of a lane's next word
+  // (32 words on) is at most a few blocks ahead, so a short linear step finds
+  // it.  Shorter blocks (1D, 2D, low rates) go straight to bisection.
+  const u32 lin = po[nb] - po[0] >= (u64)nb * 512 ? 4 : 0;
   u32 j = 0;
   for (u64 w = wbeg + lane; w < wend; w += 32) {
     u64 v = 0;
@@ -293,7 +300,19 @@ __device__ void pack_warp(const u64* slots, u64 slot_words, const u64* off, u64 
       fill = (u32)(start & 63);
       pos = start;
     }
-    while (j + 1 < nb && po[j + 1] <= pos) j++;  // the block holding bit `pos`
+    // The block holding bit `pos`: the largest j < nb with po[j] <= pos.  It
+    // only moves forward, so step from the last one; a far owner is found by
+    // bisection instead.
+    u32 steps = 0;
+    while (steps < lin && j + 1 < nb && po[j + 1] <= pos) j++, steps++;
+    if (j + 1 < nb && po[j + 1] <= pos) {
+      u32 hi = nb;
+      while (hi - j > 1) {
+        const u32 mid = (j + hi) >> 1;
+        if (po[mid] <= pos) j = mid;
+        else hi = mid;
+      }
+    }
     u64 blk = b0 + j;
     u64 pj = po[j], qj = po[j + 1];
     while (fill < 64 && blk < nblocks) {
@@ -316,13 +335,22 @@ __device__ void pack_warp(const u64* slots, u64 slot_words, const u64* off, u64 
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(256) k_pack(PackArgs a) {
-  __shared__ u64 soff[8][33];
+// Blocks per warp of the pack: more for small blocks.
+static inline int pack_blocks_per_warp(int dims) { return dims <= 2 ? 128 : 32; }
+
+template <int BW> __global__ void __launch_bounds__(256) k_pack(PackArgs a) {
+  __shared__ u64 soff[8][BW + 1];
   const u32 wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const u64 b0 = ((u64)blockIdx.x * 8 + wib) * 32;
+  const u64 b0 = ((u64)blockIdx.x * 8 + wib) * BW;
   if (b0 >= a.nblocks) return;
-  pack_warp(a.slots, a.slot_words, a.off, a.start, a.nblocks, a.start, a.init_word, a.out, ~0ull, b0, soff[wib],
-            lane);
+  pack_warp<BW>(a.slots, a.slot_words, a.off, a.start, a.nblocks, a.start, a.init_word, a.out, ~0ull, b0, soff[wib],
+                lane);
+}
+
+static cudaError_t launch_pack(const PackArgs& pa, int dims, cudaStream_t s) {
+  if (pack_blocks_per_warp(dims) == 128) k_pack<128><<<(unsigned)((pa.nblocks + 1023) / 1024), 256, 0, s>>>(pa);
+  else k_pack<32><<<(unsigned)((pa.nblocks + 255) / 256), 256, 0, s>>>(pa);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -532,9 +560,8 @@ Status compress(const Call& call, const void* d_field, u64* d_out, u64 cap, u64 
   pa.out = d_out;
   {
     KernelTimer t(K_PACK, s);
-    k_pack<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pa);
+    ZFPB_CHECK(launch_pack(pa, call.dims, s));
   }
-  ZFPB_CHECK(cudaGetLastError());
   return OK;
 }
 
@@ -967,19 +994,20 @@ static constexpr u32 BATCH_TILE = 128;
 static constexpr u64 BATCH_ROUND_BYTES = 8ull << 30;  // slot or plane scratch per round
 
 __global__ void __launch_bounds__(256) k_pack_batch(BatchArgs a) {
-  __shared__ u64 soff[8][33];
+  constexpr int BW = 128;
+  __shared__ u64 soff[8][BW + 1];
   const BatchTile t = a.tiles[blockIdx.x];
   const u32 wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const u64 b0 = t.first + (u64)wib * 32;
+  const u64 b0 = t.first + (u64)wib * BW;
   if (b0 >= t.first + t.count) return;
   const BatchItem* it = a.items + t.item;
   const u64* off = a.offsets + it->len_base;
   const u64 n = it->f.nblocks;
   const u64 delta = 0ull - off[0];
-  pack_warp(a.slots + it->slot_base, it->slot_words, off, delta, n, 0, 0, it->stream, it->stream_words, b0,
-            soff[wib], lane);
+  pack_warp<BW>(a.slots + it->slot_base, it->slot_words, off, delta, n, 0, 0, it->stream, it->stream_words, b0,
+                soff[wib], lane);
   if (it->index) {
-    const u64 e = b0 + 32 < n ? b0 + 32 : n;
+    const u64 e = b0 + BW < n ? b0 + BW : n;
     for (u64 i = b0 + lane; i < e; i += 32) it->index[i] = off[i] + delta;
     if (e == n && lane == 0) it->index[n] = off[n] + delta;
   }
@@ -1324,7 +1352,7 @@ cudaError_t build_plan(BatchPlan& P, const BatchJob* jobs, const std::vector<u32
     }
     if (P.compress) {
       R.ptile0 = (u32)P.tiles.size();
-      for (u32 k = R.item0; k < R.item0 + R.nitems; k++) append_tiles(P, k, P.items[k].f.nblocks, 256);
+      for (u32 k = R.item0; k < R.item0 + R.nitems; k++) append_tiles(P, k, P.items[k].f.nblocks, 1024);
       R.nptiles = (u32)P.tiles.size() - R.ptile0;
     }
     P.rounds.push_back(std::move(R));
@@ -1704,8 +1732,7 @@ Status compress_noalloc(const Call& call, const void* d_field, u64* d_out, u64 c
   pa.start = 0;
   pa.init_word = 0;
   pa.out = d_out;
-  k_pack<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pa);
-  ZFPB_CHECK(cudaGetLastError());
+  ZFPB_CHECK(launch_pack(pa, call.dims, s));
   ZFPB_CHECK(cudaStreamSynchronize(s));
   return OK;
 }

@@ -209,11 +209,12 @@ template <class T, int D> struct KernelShape {
   static constexpr int N = 1 << (2 * D);
   static constexpr int W = N <= 64 ? 1 : N / 64;
   static constexpr int PREC = Traits<T>::PREC;
-  // Shared-memory words of plane storage per thread.
-  static constexpr int PLANE_WORDS = PREC * W;
+  // Shared-memory words of plane storage per thread (none for 4-value
+  // blocks, whose planes stay in registers).
+  static constexpr int PLANE_WORDS = D == 1 ? 0 : PREC * W;
   // CTAs of 128 threads per SM the register allocation must allow: 4 caps
-  // 32-bit blocks at 128 registers (16 warps per SM), 2 caps 64-bit ones at
-  // 255.  Occupancy hides the latency of the sequential bit-plane coding.
+  // 32-bit blocks at 128 registers (16 warps per SM), 3 caps 64-bit ones at
+  // 168.  Occupancy hides the latency of the sequential bit-plane coding.
   static constexpr int MIN_CTAS = sizeof(T) == 4 ? 4 : 3;
 };
 
