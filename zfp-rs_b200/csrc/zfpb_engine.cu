@@ -159,6 +159,7 @@ int timing_read(double* ms, unsigned long long* counts, int n) {
 static constexpr int SCAN_THREADS = 256;
 static constexpr int SCAN_ITEMS = 8;
 static constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+static_assert(SCAN_ITEMS == 8, "scan_load reads two uint4");
 
 // Block-wide inclusive scan of one u64 per thread (warp shuffles + smem).
 __device__ __forceinline__ u64 block_inclusive_scan(u64 v, u64* warp_sums) {
@@ -186,13 +187,27 @@ __device__ __forceinline__ u64 block_inclusive_scan(u64 v, u64* warp_sums) {
   return v;
 }
 
+// A thread's SCAN_ITEMS lengths: two 16-byte loads where the run is whole
+// and aligned, else one at a time.
+__device__ __forceinline__ void scan_load(const u32* len, u64 n, u64 base, u32* v) {
+  const u32* p = len + base;
+  if (base + SCAN_ITEMS <= n && ((uintptr_t)p & 15) == 0) {
+    const uint4 a = reinterpret_cast<const uint4*>(p)[0], b = reinterpret_cast<const uint4*>(p)[1];
+    v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+  } else {
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++) v[i] = base + i < n ? len[base + i] : 0u;
+  }
+}
+
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const u32* len, u64 n, u64* partial) {
   __shared__ u64 ws[32];
   const u64 base = (u64)blockIdx.x * SCAN_TILE + (u64)threadIdx.x * SCAN_ITEMS;
+  u32 v[SCAN_ITEMS];
+  scan_load(len, n, base, v);
   u64 s = 0;
 #pragma unroll
-  for (int i = 0; i < SCAN_ITEMS; i++)
-    if (base + i < n) s += len[base + i];
+  for (int i = 0; i < SCAN_ITEMS; i++) s += v[i];
   u64 incl = block_inclusive_scan(s, ws);
   if (threadIdx.x == blockDim.x - 1) partial[blockIdx.x] = incl;
 }
@@ -220,19 +235,27 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(const u32* len, u64
                                                               u64* off) {
   __shared__ u64 ws[32];
   const u64 base = (u64)blockIdx.x * SCAN_TILE + (u64)threadIdx.x * SCAN_ITEMS;
-  u64 v[SCAN_ITEMS];
+  u32 v[SCAN_ITEMS];
+  scan_load(len, n, base, v);
   u64 s = 0;
 #pragma unroll
-  for (int i = 0; i < SCAN_ITEMS; i++) {
-    v[i] = base + i < n ? len[base + i] : 0;
-    s += v[i];
-  }
+  for (int i = 0; i < SCAN_ITEMS; i++) s += v[i];
   u64 incl = block_inclusive_scan(s, ws);
   u64 run = partial[blockIdx.x] + incl - s;
+  u64 o[SCAN_ITEMS];
 #pragma unroll
   for (int i = 0; i < SCAN_ITEMS; i++) {
-    if (base + i < n) off[base + i] = run;
+    o[i] = run;
     run += v[i];
+  }
+  u64* q = off + base;
+  if (base + SCAN_ITEMS <= n && ((uintptr_t)q & 15) == 0) {
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i += 2) reinterpret_cast<ulonglong2*>(q)[i / 2] = make_ulonglong2(o[i], o[i + 1]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++)
+      if (base + i < n) q[i] = o[i];
   }
 }
 
@@ -261,10 +284,9 @@ struct PackArgs {
   u64* out;
 };
 
-__device__ __forceinline__ u64 slot_bits(const u64* slot, u64 local, u32 take) {
+__device__ __forceinline__ u64 slot_bits(const u64* slot, u32 local, u32 take) {
   if (take == 0) return 0;
-  u64 wi = local >> 6;
-  u32 sh = (u32)(local & 63);
+  const u32 wi = local >> 6, sh = local & 63;
   u64 x = slot[wi] >> sh;
   if (sh != 0 && take > 64 - sh) x |= slot[wi + 1] << (64 - sh);
   return take < 64 ? x & ((1ull << take) - 1) : x;
@@ -274,31 +296,36 @@ __device__ __forceinline__ u64 slot_bits(const u64* slot, u64 local, u32 take) {
 // of stream words; lane l assembles words l, l + 32, ... of that run, finding
 // each word's owner among the warp's block offsets (kept in shared memory), so
 // slot reads and stream writes are coalesced and the lanes' loads do not wait
-// on one another.  A word that runs past its owner's end
-// takes the rest of its bits from the blocks after it.  Block i's bits start
-// at delta + off[i]; only words below `cap` are written.  Small blocks (1D,
-// 2D) use more blocks per warp so that a warp has enough words to share out.
+// on one another.  A word that runs past its owner's end takes the rest of its
+// bits from the blocks after it.  Block i's bits start at delta + off[i]; only
+// words below `cap` are written.  Bit positions inside the warp's run are
+// 32-bit, relative to its first block (BW blocks of at most ZFP's largest
+// block, 4^4 doubles, span far less than 2^32 bits).  Small blocks (1D, 2D)
+// use more blocks per warp so that a warp has enough words to share out.
 template <int BW>
 __device__ void pack_warp(const u64* slots, u64 slot_words, const u64* off, u64 delta, u64 nblocks, u64 start,
-                          u64 init_word, u64* out, u64 cap, u64 b0, u64* po, u32 lane) {
+                          u64 init_word, u64* out, u64 cap, u64 b0, u32* po, u32 lane) {
   const u32 nb = (u32)(nblocks - b0 < BW ? nblocks - b0 : BW);
-  for (u32 t = lane; t <= nb; t += 32) po[t] = delta + off[b0 + t];
+  const u64 base = delta + off[b0];  // bit of the warp's first block; == start when b0 == 0
+  for (u32 t = lane; t <= nb; t += 32) po[t] = (u32)(delta + off[b0 + t] - base);
   __syncwarp();
-  const u64 wbeg = b0 == 0 ? start >> 6 : (po[0] + 63) >> 6;
-  const u64 wend = (po[nb] + 63) >> 6;
+  const u32 span = po[nb];
+  const u64 wbeg = b0 == 0 ? start >> 6 : (base + 63) >> 6;
+  const u64 wend = (base + span + 63) >> 6;
   // Blocks of 8 words or more on average: the owner of a lane's next word
   // (32 words on) is at most a few blocks ahead, so a short linear step finds
   // it.  Shorter blocks (1D, 2D, low rates) go straight to bisection.
-  const u32 lin = po[nb] - po[0] >= (u64)nb * 512 ? 4 : 0;
+  const u32 lin = span >= nb * 512u ? 4 : 0;
   u32 j = 0;
   for (u64 w = wbeg + lane; w < wend; w += 32) {
     u64 v = 0;
-    u32 fill = 0;
-    u64 pos = w << 6;
-    if (b0 == 0 && w == (start >> 6)) {
+    u32 fill = 0, pos;
+    if (b0 == 0 && w == wbeg) {
       v = init_word;
       fill = (u32)(start & 63);
-      pos = start;
+      pos = 0;
+    } else {
+      pos = (u32)((w << 6) - base);
     }
     // The block holding bit `pos`: the largest j < nb with po[j] <= pos.  It
     // only moves forward, so step from the last one; a far owner is found by
@@ -313,20 +340,38 @@ __device__ void pack_warp(const u64* slots, u64 slot_words, const u64* off, u64 
         else hi = mid;
       }
     }
-    u64 blk = b0 + j;
-    u64 pj = po[j], qj = po[j + 1];
-    while (fill < 64 && blk < nblocks) {
-      u64 local = pos - pj;
-      u64 avail = qj - pos;
-      u32 take = (u32)(avail < (u64)(64 - fill) ? avail : (u64)(64 - fill));
-      v |= slot_bits(slots + blk * slot_words, local, take) << fill;  // fill < 64
+    u32 jj = j;
+    u32 pj = po[jj], qj = po[jj + 1];
+    while (fill < 64 && jj < nb) {
+      const u32 avail = qj - pos;
+      const u32 take = avail < 64 - fill ? avail : 64 - fill;
+      v |= slot_bits(slots + (b0 + jj) * slot_words, pos - pj, take) << fill;  // fill < 64
       fill += take;
       pos += take;
       if (pos == qj) {
-        blk++;
-        if (blk < nblocks) {
-          pj = qj;
-          qj = delta + off[blk + 1];
+        jj++;
+        pj = qj;
+        qj = po[jj + (jj < nb)];  // past the last block: loop ends
+      }
+    }
+    // A word that runs past the warp's blocks takes the rest from the next
+    // warp's (only the run's last word; never for the array's last block).
+    if (fill < 64 && b0 + nb < nblocks) {
+      u64 blk = b0 + nb;
+      u64 pj64 = base + span, qj64 = delta + off[blk + 1];
+      u64 pos64 = base + pos;
+      while (fill < 64 && blk < nblocks) {
+        const u64 avail = qj64 - pos64;
+        const u32 take = (u32)(avail < (u64)(64 - fill) ? avail : (u64)(64 - fill));
+        v |= slot_bits(slots + blk * slot_words, (u32)(pos64 - pj64), take) << fill;
+        fill += take;
+        pos64 += take;
+        if (pos64 == qj64) {
+          blk++;
+          if (blk < nblocks) {
+            pj64 = qj64;
+            qj64 = delta + off[blk + 1];
+          }
         }
       }
     }
@@ -339,7 +384,7 @@ __device__ void pack_warp(const u64* slots, u64 slot_words, const u64* off, u64 
 static inline int pack_blocks_per_warp(int dims) { return dims <= 2 ? 128 : 32; }
 
 template <int BW> __global__ void __launch_bounds__(256) k_pack(PackArgs a) {
-  __shared__ u64 soff[8][BW + 1];
+  __shared__ u32 soff[8][BW + 1];
   const u32 wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const u64 b0 = ((u64)blockIdx.x * 8 + wib) * BW;
   if (b0 >= a.nblocks) return;
@@ -724,7 +769,7 @@ __global__ void __launch_bounds__(256) k_pack_range(PackArgs a, u64 wa, u64 wb) 
     const u64 local = pos - pj;
     const u64 avail = qj - pos;
     const u32 take = (u32)(avail < (u64)(64 - fill) ? avail : (u64)(64 - fill));
-    v |= slot_bits(a.slots + blk * a.slot_words, local, take) << fill;
+    v |= slot_bits(a.slots + blk * a.slot_words, (u32)local, take) << fill;  // local < a slot
     fill += take;
     pos += take;
     if (pos == qj) {
@@ -995,7 +1040,7 @@ static constexpr u64 BATCH_ROUND_BYTES = 8ull << 30;  // slot or plane scratch p
 
 __global__ void __launch_bounds__(256) k_pack_batch(BatchArgs a) {
   constexpr int BW = 128;
-  __shared__ u64 soff[8][BW + 1];
+  __shared__ u32 soff[8][BW + 1];
   const BatchTile t = a.tiles[blockIdx.x];
   const u32 wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const u64 b0 = t.first + (u64)wib * BW;
