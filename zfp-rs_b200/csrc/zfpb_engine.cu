@@ -392,9 +392,90 @@ template <int BW> __global__ void __launch_bounds__(256) k_pack(PackArgs a) {
                 lane);
 }
 
+// Staged pack for small blocks (slots of at most STAGE_SLOT_WORDS words: 1D
+// blocks, 2D blocks of 32-bit values).  A CTA takes STAGE_BLOCKS consecutive
+// blocks; each thread ORs its blocks' bits into a shared copy of the stream
+// words they cover, then the CTA stores the words it owns (those whose first
+// bit lies in its blocks' range; the first CTA also owns the word holding
+// `start`) in coalesced runs.  The last owned word takes the rest of its bits
+// from the blocks after the CTA's.  Where a warp per word spends most of its
+// time finding each word's owner among many short blocks, here a block costs
+// a load and two shared-memory ORs per slot word.
+static constexpr u32 STAGE_BLOCKS = 512;
+static constexpr u64 STAGE_SLOT_WORDS = 10;
+
+struct StageSmem {
+  u64 buf[STAGE_BLOCKS * (STAGE_SLOT_WORDS - 1) + 2];  // a block has at most (slot_words - 1) * 64 bits
+  u32 po[STAGE_BLOCKS + 1];
+};
+
+__device__ void pack_stage(const u64* slots, u64 slot_words, const u64* off, u64 delta, u64 nblocks, u64 start,
+                           u64 init_word, u64* out, u64 cap, u64 b0, StageSmem& sm) {
+  const u32 tid = threadIdx.x, nt = blockDim.x;
+  const u32 nb = (u32)(nblocks - b0 < STAGE_BLOCKS ? nblocks - b0 : STAGE_BLOCKS);
+  const u64 base = delta + off[b0];  // == start when b0 == 0
+  for (u32 t = tid; t <= nb; t += nt) sm.po[t] = (u32)(delta + off[b0 + t] - base);
+  const u32 s0 = (u32)(base & 63);
+  const u64 wfirst = base >> 6;  // global index of buffer word 0
+  __syncthreads();
+  const u32 span = sm.po[nb];
+  const u32 nwords = (s0 + span + 63) >> 6;
+  for (u32 i = tid; i < nwords; i += nt) sm.buf[i] = (i == 0 && b0 == 0) ? init_word : 0ull;
+  __syncthreads();
+  for (u32 i = tid; i < nb; i += nt) {
+    const u32 p = s0 + sm.po[i], len = sm.po[i + 1] - sm.po[i];
+    const u64* slot = slots + (b0 + i) * slot_words;
+    for (u32 k = 0; k * 64 < len; k++) {
+      u64 x = slot[k];
+      const u32 take = len - k * 64;
+      if (take < 64) x &= (1ull << take) - 1;
+      const u32 q = p + k * 64, wi = q >> 6, sh = q & 63;
+      atomicOr(&sm.buf[wi], x << sh);
+      if (sh != 0 && (x >> (64 - sh)) != 0) atomicOr(&sm.buf[wi + 1], x >> (64 - sh));
+    }
+  }
+  __syncthreads();
+  const u32 first = (b0 == 0 || s0 == 0) ? 0 : 1;  // else word 0 is the previous CTA's
+  for (u32 wi = first + tid; wi < nwords; wi += nt) {
+    u64 v = sm.buf[wi];
+    u32 fill = (s0 + span) & 63;
+    if (wi == nwords - 1 && fill != 0 && b0 + nb < nblocks) {
+      // The rest of the word from the blocks after this CTA's.
+      u64 blk = b0 + nb;
+      u64 pj = base + span, qj = delta + off[blk + 1], pos = pj;
+      while (fill < 64 && blk < nblocks) {
+        const u64 avail = qj - pos;
+        const u32 take = (u32)(avail < (u64)(64 - fill) ? avail : (u64)(64 - fill));
+        v |= slot_bits(slots + blk * slot_words, (u32)(pos - pj), take) << fill;
+        fill += take;
+        pos += take;
+        if (pos == qj) {
+          blk++;
+          if (blk < nblocks) {
+            pj = qj;
+            qj = delta + off[blk + 1];
+          }
+        }
+      }
+    }
+    const u64 g = wfirst + wi;
+    if (g < cap) out[g] = v;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_pack_stage(PackArgs a) {
+  __shared__ StageSmem sm;
+  pack_stage(a.slots, a.slot_words, a.off, a.start, a.nblocks, a.start, a.init_word, a.out, ~0ull,
+             (u64)blockIdx.x * STAGE_BLOCKS, sm);
+}
+
 static cudaError_t launch_pack(const PackArgs& pa, int dims, cudaStream_t s) {
-  if (pack_blocks_per_warp(dims) == 128) k_pack<128><<<(unsigned)((pa.nblocks + 1023) / 1024), 256, 0, s>>>(pa);
-  else k_pack<32><<<(unsigned)((pa.nblocks + 255) / 256), 256, 0, s>>>(pa);
+  if (pa.slot_words <= STAGE_SLOT_WORDS)
+    k_pack_stage<<<(unsigned)((pa.nblocks + STAGE_BLOCKS - 1) / STAGE_BLOCKS), 256, 0, s>>>(pa);
+  else if (pack_blocks_per_warp(dims) == 128)
+    k_pack<128><<<(unsigned)((pa.nblocks + 1023) / 1024), 256, 0, s>>>(pa);
+  else
+    k_pack<32><<<(unsigned)((pa.nblocks + 255) / 256), 256, 0, s>>>(pa);
   return cudaGetLastError();
 }
 
@@ -1038,23 +1119,33 @@ Status decompress_host(const Call& call, const u64* h_in, u64* d_in, u64 len, u6
 static constexpr u32 BATCH_TILE = 128;
 static constexpr u64 BATCH_ROUND_BYTES = 8ull << 30;  // slot or plane scratch per round
 
+// A tile of at most STAGE_BLOCKS blocks of one array: the staged pack for
+// small slots, else a warp per BW = STAGE_BLOCKS / 8 blocks.
 __global__ void __launch_bounds__(256) k_pack_batch(BatchArgs a) {
-  constexpr int BW = 128;
-  __shared__ u32 soff[8][BW + 1];
+  constexpr int BW = STAGE_BLOCKS / 8;
+  __shared__ union {
+    StageSmem stage;
+    u32 soff[8][BW + 1];
+  } sm;
   const BatchTile t = a.tiles[blockIdx.x];
-  const u32 wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const u64 b0 = t.first + (u64)wib * BW;
-  if (b0 >= t.first + t.count) return;
   const BatchItem* it = a.items + t.item;
   const u64* off = a.offsets + it->len_base;
   const u64 n = it->f.nblocks;
   const u64 delta = 0ull - off[0];
-  pack_warp<BW>(a.slots + it->slot_base, it->slot_words, off, delta, n, 0, 0, it->stream, it->stream_words, b0,
-                soff[wib], lane);
+  if (it->slot_words <= STAGE_SLOT_WORDS) {
+    pack_stage(a.slots + it->slot_base, it->slot_words, off, delta, n, 0, 0, it->stream, it->stream_words, t.first,
+               sm.stage);
+  } else {
+    const u32 wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const u64 b0 = t.first + (u64)wib * BW;
+    if (b0 < t.first + t.count)
+      pack_warp<BW>(a.slots + it->slot_base, it->slot_words, off, delta, n, 0, 0, it->stream, it->stream_words, b0,
+                    sm.soff[wib], lane);
+  }
   if (it->index) {
-    const u64 e = b0 + BW < n ? b0 + BW : n;
-    for (u64 i = b0 + lane; i < e; i += 32) it->index[i] = off[i] + delta;
-    if (e == n && lane == 0) it->index[n] = off[n] + delta;
+    const u64 e = t.first + t.count;
+    for (u64 i = t.first + threadIdx.x; i < e; i += blockDim.x) it->index[i] = off[i] + delta;
+    if (e == n && threadIdx.x == 0) it->index[n] = off[n] + delta;
   }
 }
 
@@ -1397,7 +1488,7 @@ cudaError_t build_plan(BatchPlan& P, const BatchJob* jobs, const std::vector<u32
     }
     if (P.compress) {
       R.ptile0 = (u32)P.tiles.size();
-      for (u32 k = R.item0; k < R.item0 + R.nitems; k++) append_tiles(P, k, P.items[k].f.nblocks, 1024);
+      for (u32 k = R.item0; k < R.item0 + R.nitems; k++) append_tiles(P, k, P.items[k].f.nblocks, STAGE_BLOCKS);
       R.nptiles = (u32)P.tiles.size() - R.ptile0;
     }
     P.rounds.push_back(std::move(R));
