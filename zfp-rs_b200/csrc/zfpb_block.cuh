@@ -1418,6 +1418,29 @@ ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 in
       }
     }
     k--;
+    if constexpr (N == 16 || N == 64) {
+      // At most 4 coefficients still insignificant: the plane's code is its
+      // first size - 4 bits verbatim, then the code of a 4-value plane with
+      // n - (size - 4) significant (the group tests depend only on how many
+      // coefficients remain), which the 4-value table reads.  (The encoder
+      // keeps its general path here: the table made it slower.)
+      constexpr u32 P = size - 4;
+      if (n >= P && n < size) {
+        const u64 t = WIDE ? (lo >> P) | (r.hi() << (64 - P)) : lo >> P;
+        const u32 e = kPlane4.dec[(n - P) * 256 + (u32)(t & 0xff)];
+        const u32 len = (e >> 4) & 15u;
+        if (len != 0 && P + len <= bits) {
+          ps.at(k, 0, 1) = (lo & low_mask(P)) | ((u64)(e & 15u) << P);
+          if (high < 0) high = (int)k;
+          low = (int)k;
+          n = P + (e >> 8);
+          m = size;
+          bits -= P + len;
+          r.advance(P + len);
+          continue;
+        }
+      }
+    }
     if constexpr (N == 4) {
       const u32 e = kPlane4.dec[n * 256 + (u32)(lo & 0xff)];
       const u32 len = (e >> 4) & 15u;
@@ -1812,6 +1835,20 @@ ZFPB_DEV u32 plane_bits(Reader& rd, u32 budget, u32 kmin, u32 intprec) {
       }
     }
     k--;
+    if constexpr (N == 16 || N == 64) {
+      constexpr u32 P = size - 4;  // as in decode_planes_sync
+      if (n >= P) {
+        const u64 t = WIDE ? (lo >> P) | (r.hi() << (64 - P)) : lo >> P;
+        const u32 e = kPlane4.dec[(n - P) * 256 + (u32)(t & 0xff)];
+        const u32 len = (e >> 4) & 15u;
+        if (len != 0 && P + len <= bits) {
+          n = P + (e >> 8);
+          bits -= P + len;
+          r.advance(P + len);
+          continue;
+        }
+      }
+    }
     if constexpr (N == 4) {
       const u32 e = kPlane4.dec[n * 256 + (u32)(lo & 0xff)];
       const u32 len = (e >> 4) & 15u;
