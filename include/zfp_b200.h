@@ -23,7 +23,7 @@ int zfp_stream_rounding(const zfp_stream* stream, zfp_bool* tight_error);
 
 /* Status of the last failed call on this thread: 0 none, 1 buffer too small,
  * 2 truncated stream, 3 CUDA error, 4 invalid arguments, 6 field too large
- * for zfpb_compress_device_noalloc. */
+ * for zfpb_compress_device_noalloc, 7 a batch item's stream lacks its header. */
 int zfpb_last_error(void);
 
 /* A field and codec parameters in one plain struct for the device API. */
@@ -95,13 +95,19 @@ typedef struct zfpb_batch_item {
   void* d_stream;             /* 8-byte aligned; compress: written from bit 0; decompress: read */
   size_t stream_bytes;        /* compress: capacity; decompress: stream size */
   uint64_t* d_block_offsets;  /* optional nblocks + 1 block offsets, as for zfpb_compress_device:
-                                 compress writes them, decompress uses them if they match */
-  size_t result;              /* out: stream bytes written / consumed, 0 on failure */
+                                 compress writes them, decompress uses them if they match;
+                                 relative to the first block (after the header, if any) */
+  uint header_mask;           /* ZFP_HEADER_* bits, 0 = none.  Compress: the stream begins with
+                                 the zfp_write_header(mask) header of desc's field and mode;
+                                 decompress: the stream must begin with that header (else
+                                 status 7 and result 0), and the blocks follow it */
+  size_t result;              /* out: stream bytes written / consumed (header included), 0 on failure */
   int status;                 /* out: 0, or the zfpb_last_error code of this item */
 } zfpb_batch_item;
 
-/* Compress / decompress every item (stream from bit 0, no header).  Returns
- * the number of items that succeeded; the call returns once all are done. */
+/* Compress / decompress every item (blocks from bit 0, or after the item's
+ * header).  Returns the number of items that succeeded; the call returns once
+ * all are done. */
 size_t zfpb_compress_batch(zfpb_batch_item* items, size_t n, void* cuda_stream);
 size_t zfpb_decompress_batch(zfpb_batch_item* items, size_t n, void* cuda_stream);
 

@@ -133,6 +133,48 @@ def test_batch_streams_match_oracle():
         assert streams[i][: n // 8].cpu().numpy().tobytes() == want
 
 
+def test_batch_headers_match_oracle_and_are_checked():
+    """Items whose streams carry a zfp header (full, mode only, magic + meta,
+    magic only, none): each stream is the oracle's header-then-blocks stream,
+    decompress reads the blocks after the header (with the index, and by
+    walking without it), and a stream whose header does not match its
+    description fails with status 7 while the other items decode."""
+    import torch
+
+    jobs = mixed_jobs(4, n=15)
+    ref = single(jobs)
+    streams, offsets = batch_buffers(jobs)
+    fields = [x for x, _ in jobs]
+    cfgs = [c for _, c in jobs]
+    masks = [[7, 0, 4, 3, 1][i % 5] for i in range(len(jobs))]
+    items = Z.batch_items(fields, cfgs, streams, offsets=offsets, header_mask=masks)
+    sizes = Z.compress_batch(items)
+    for i, (x, cfg) in enumerate(jobs):
+        want, n = orc.compress(x.cpu().numpy(), orc.config(cfg.min_bits, cfg.max_bits, cfg.max_prec, cfg.min_exp,
+                                                          cfg.rounding, cfg.tight_error), header_mask=masks[i])
+        assert sizes[i] == n, (i, masks[i])
+        assert streams[i][: n // 8].cpu().numpy().tobytes() == want, (i, masks[i], cfg)
+    for use_index in (True, False):
+        outs = [torch.full_like(x, 7) for x in fields]
+        used = Z.decompress_batch(Z.batch_items(outs, cfgs, streams, nbytes=sizes,
+                                                offsets=offsets if use_index else None, header_mask=masks))
+        for i, (_, y) in enumerate(ref):
+            assert used[i] == sizes[i]
+            assert torch.equal(outs[i].view(torch.uint8), y.view(torch.uint8)), (use_index, i, masks[i])
+    bad = masks.index(7)
+    streams[bad][0] ^= 1  # the magic's first byte
+    outs = [torch.full_like(x, 7) for x in fields]
+    ditems = Z.batch_items(outs, cfgs, streams, nbytes=sizes, offsets=offsets, header_mask=masks)
+    ok = Z.lib().zfpb_decompress_batch(ditems, len(ditems), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert ok == len(ditems) - 1
+    assert ditems[bad].status == 7 and ditems[bad].result == 0
+    for i, (_, y) in enumerate(ref):
+        if i != bad:
+            assert ditems[i].status == 0 and ditems[i].result == sizes[i]
+            assert torch.equal(outs[i].view(torch.uint8), y.view(torch.uint8)), i
+
+
 def test_batch_reports_overflow_and_bad_index_per_item():
     import torch
 

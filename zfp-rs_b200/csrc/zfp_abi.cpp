@@ -1326,6 +1326,49 @@ extern "C" size_t zfpb_decompress_device(const zfpb_desc* d, const void* d_strea
   return (size_t)((end + 63) / 64 * 8);
 }
 
+// The header zfp_write_header(mask) writes for a description's field and mode:
+// its words (zero past the last bit) and its length in bits.  False if the
+// description has none (e.g. sizes the metadata cannot hold).
+static bool header_of_desc(const zfpb_desc* d, uint mask, u64* hdr, u64* bits) {
+  hdr[0] = hdr[1] = hdr[2] = 0;
+  *bits = 0;
+  if (!mask) return true;
+  zfp_field f;
+  memset(&f, 0, sizeof(f));
+  f.type = d->type;
+  f.nx = d->nx; f.ny = d->ny; f.nz = d->nz; f.nw = d->nw;
+  zfp_stream zs;
+  memset(&zs, 0, sizeof(zs));
+  zs.minbits = d->minbits;
+  zs.maxbits = d->maxbits;
+  zs.maxprec = d->maxprec;
+  zs.minexp = d->minexp;
+  alignas(8) u64 buf[4] = {0, 0, 0, 0};
+  bitstream* bs = stream_open(buf, sizeof(buf));
+  if (!bs) return false;
+  zs.stream = bs;
+  const size_t n = zfp_write_header(&zs, &f, mask);
+  stream_flush(bs);
+  stream_close(bs);
+  if (n == 0 || n > 3 * 64) return false;
+  for (int w = 0; w < 3; w++) hdr[w] = buf[w];
+  *bits = n;
+  return true;
+}
+
+// An item's job: its call, buffers and header.
+static bool job_of_item(const zfpb_batch_item& it, zfpb::BatchJob& J) {
+  if (!it.d_field || !it.d_stream || ((uintptr_t)it.d_stream % 8) != 0) return false;
+  Plan p;
+  if (!call_of_desc(&it.desc, p, J.call, it.d_field)) return false;
+  if (!header_of_desc(&it.desc, it.header_mask, J.hdr, &J.start_bit)) return false;
+  J.field = it.d_field;
+  J.stream = (u64*)it.d_stream;
+  J.stream_words = it.stream_bytes / 8;
+  J.index = (u64*)it.d_block_offsets;
+  return true;
+}
+
 // Batches: every item converted to an engine job, coded together
 // (zfpb::compress_batch / decompress_batch), results written back per item.
 static size_t run_batch_abi(zfpb_batch_item* items, size_t n, void* cuda_stream, bool compress) {
@@ -1337,14 +1380,7 @@ static size_t run_batch_abi(zfpb_batch_item* items, size_t n, void* cuda_stream,
     zfpb_batch_item& it = items[i];
     it.result = 0;
     it.status = zfpb::ERR_ARGS;
-    if (!it.d_field || !it.d_stream || ((uintptr_t)it.d_stream % 8) != 0) continue;
-    Plan p;
-    zfpb::BatchJob& J = jobs[m];
-    if (!call_of_desc(&it.desc, p, J.call, it.d_field)) continue;
-    J.field = it.d_field;
-    J.stream = (u64*)it.d_stream;
-    J.stream_words = it.stream_bytes / 8;
-    J.index = (u64*)it.d_block_offsets;
+    if (!job_of_item(it, jobs[m])) continue;
     job_of[i] = m++;
   }
   cudaStream_t s = (cudaStream_t)cuda_stream;
@@ -1387,14 +1423,9 @@ extern "C" zfpb_server* zfpb_server_create(size_t budget_bytes, int lanes, size_
 }
 
 extern "C" int zfpb_server_submit(zfpb_server* srv, const zfpb_batch_item* it, int decompress, uint64_t tag) {
-  if (!srv || !it || !it->d_field || !it->d_stream || ((uintptr_t)it->d_stream % 8) != 0) return fail(zfpb::ERR_ARGS);
-  Plan p;
+  if (!srv || !it) return fail(zfpb::ERR_ARGS);
   zfpb::BatchJob J{};
-  if (!call_of_desc(&it->desc, p, J.call, it->d_field)) return fail(zfpb::ERR_ARGS);
-  J.field = it->d_field;
-  J.stream = (u64*)it->d_stream;
-  J.stream_words = it->stream_bytes / 8;
-  J.index = (u64*)it->d_block_offsets;
+  if (!job_of_item(*it, J)) return fail(zfpb::ERR_ARGS);
   if (!zfpb::server_submit(reinterpret_cast<zfpb::Server*>(srv), J, decompress != 0, tag))
     return fail(zfpb::ERR_TOO_LARGE);
   return 1;

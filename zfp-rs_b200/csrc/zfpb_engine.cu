@@ -1131,16 +1131,19 @@ __global__ void __launch_bounds__(256) k_pack_batch(BatchArgs a) {
   const BatchItem* it = a.items + t.item;
   const u64* off = a.offsets + it->len_base;
   const u64 n = it->f.nblocks;
-  const u64 delta = 0ull - off[0];
+  const u64 delta = 0ull - off[0];  // block offsets relative to the first block
+  // The blocks follow the header: from bit it->start, whose word holds the
+  // header's last bits (k_batch_ends writes its whole words).
+  const u64 start = it->start, init_word = it->hdr[start >> 6];
   if (it->slot_words <= STAGE_SLOT_WORDS) {
-    pack_stage(a.slots + it->slot_base, it->slot_words, off, delta, n, 0, 0, it->stream, it->stream_words, t.first,
-               sm.stage);
+    pack_stage(a.slots + it->slot_base, it->slot_words, off, delta + start, n, start, init_word, it->stream,
+               it->stream_words, t.first, sm.stage);
   } else {
     const u32 wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const u64 b0 = t.first + (u64)wib * BW;
     if (b0 < t.first + t.count)
-      pack_warp<BW>(a.slots + it->slot_base, it->slot_words, off, delta, n, 0, 0, it->stream, it->stream_words, b0,
-                    sm.soff[wib], lane);
+      pack_warp<BW>(a.slots + it->slot_base, it->slot_words, off, delta + start, n, start, init_word, it->stream,
+                    it->stream_words, b0, sm.soff[wib], lane);
   }
   if (it->index) {
     const u64 e = t.first + t.count;
@@ -1151,6 +1154,9 @@ __global__ void __launch_bounds__(256) k_pack_batch(BatchArgs a) {
 
 // End bit of each item of [first, first + n): compress from the scanned
 // lengths; decompress from i * maxbits, the walker's offsets or the index.
+// Items with a header: compress writes its whole words (the pack wrote its
+// last, partial one with the first blocks); decompress checks the stream
+// holds it (else FLAG_BAD_HEADER).
 __global__ void k_batch_ends(BatchArgs a, u32 first, u32 n, int compress, u64* ends) {
   const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -1161,7 +1167,20 @@ __global__ void k_batch_ends(BatchArgs a, u32 first, u32 n, int compress, u64* e
   else if (it->fixed) e = nb * (u64)it->c.maxbits;
   else if (it->walk) e = a.offsets[it->len_base + nb];
   else e = it->index[nb];
-  ends[first + i] = e;
+  ends[first + i] = it->start + e;
+  const u64 hw = it->start >> 6, hb = it->start & 63;
+  if (compress) {
+    for (u64 w = 0; w < hw && w < it->stream_words; w++) it->stream[w] = it->hdr[w];
+  } else if (it->start) {
+    bool ok = true;
+    for (u64 w = 0; w <= hw && w < 3; w++) {
+      if (w == hw && hb == 0) break;
+      const u64 v = w < it->stream_words ? it->stream[w] : 0ull;
+      const u64 m = w < hw ? ~0ull : (1ull << hb) - 1;
+      ok = ok && (v & m) == it->hdr[w];
+    }
+    if (!ok) atomicOr(a.flags + first + i, FLAG_BAD_HEADER);
+  }
 }
 
 namespace {
@@ -1434,6 +1453,8 @@ cudaError_t build_plan(BatchPlan& P, const BatchJob* jobs, const std::vector<u32
       it.stream_words = J.stream_words;
       it.index = J.index;
       it.fixed = fixed_size_blocks(J.call) ? 1 : 0;
+      it.start = J.start_bit;
+      for (int w = 0; w < 3; w++) it.hdr[w] = J.hdr[w];
       it.len_base = entries;
       entries += J.call.f.nblocks + 1;
       if (P.compress) {
@@ -1558,6 +1579,8 @@ void collect(const BatchPlan& P, BatchJob* jobs, bool compress, std::vector<u32>
     const unsigned fl = P.h_flags[k];
     if (compress) {
       if ((J.end_bit + 63) / 64 > J.stream_words) J.status = ERR_OVERFLOW;
+    } else if (fl & FLAG_BAD_HEADER) {
+      J.status = ERR_HEADER;
     } else if (fl & FLAG_BAD_INDEX) {
       single.push_back(P.job_of_item[k]);
     } else if (fl & FLAG_TRUNCATED) {
@@ -1566,12 +1589,31 @@ void collect(const BatchPlan& P, BatchJob* jobs, bool compress, std::vector<u32>
   }
 }
 
+// Whether a job's stream begins with its header (for jobs decoded alone;
+// batched ones are checked by k_batch_ends).
+static bool header_matches(const BatchJob& J, cudaStream_t s) {
+  if (J.start_bit == 0) return true;
+  const u64 hw = (J.start_bit + 63) / 64;
+  if (hw > J.stream_words) return false;
+  u64 w[3] = {0, 0, 0};
+  if (cudaMemcpyAsync(w, J.stream, hw * sizeof(u64), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return false;
+  if (J.start_bit & 63) w[hw - 1] &= (1ull << (J.start_bit & 63)) - 1;
+  for (u64 i = 0; i < hw; i++)
+    if (w[i] != J.hdr[i]) return false;
+  return true;
+}
+
 // Jobs run alone: decompress without an index (compress never needs it).
 Status finish_jobs(BatchJob* jobs, size_t n, bool compress, const std::vector<u32>& single, cudaStream_t s) {
   for (u32 i : single) {
     BatchJob& J = jobs[i];
     u64 end = 0;
-    Status st = compress ? ERR_ARGS : decompress(J.call, J.stream, J.stream_words, 0, J.field, &end, nullptr, s);
+    Status st;
+    if (compress) st = ERR_ARGS;
+    else if (!header_matches(J, s)) st = ERR_HEADER;
+    else st = decompress(J.call, J.stream, J.stream_words, J.start_bit, J.field, &end, nullptr, s);
     J.status = st;
     J.end_bit = end;
   }

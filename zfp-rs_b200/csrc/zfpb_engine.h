@@ -22,7 +22,7 @@ struct FieldGeom {
   int vec_ok;  // full-block rows are 16-byte aligned contiguous runs
 };
 
-enum : unsigned { FLAG_TRUNCATED = 1u, FLAG_BAD_INDEX = 2u };
+enum : unsigned { FLAG_TRUNCATED = 1u, FLAG_BAD_INDEX = 2u, FLAG_BAD_HEADER = 4u };
 
 struct CodecParams {
   u32 minbits, maxbits, maxprec;
@@ -90,7 +90,9 @@ enum Status : int { OK = 0, ERR_OVERFLOW = 1, ERR_TRUNCATED = 2, ERR_CUDA = 3, E
                    // Candidate block offsets did not match the stream; call again without them.
                    ERR_BAD_INDEX = 5,
                    // The field needs more scratch than the no-allocation entry point has.
-                   ERR_TOO_LARGE = 6 };
+                   ERR_TOO_LARGE = 6,
+                   // A batch item's stream does not begin with the header its description gives.
+                   ERR_HEADER = 7 };
 
 // Whether every block takes exactly c.maxbits bits (minbits == maxbits and no
 // block can exceed the budget, zfp-rs config.rs:670-686).
@@ -147,6 +149,8 @@ struct BatchItem {
   u64 plane_base;    // 3D decompress: column of block 0 in the plane scratch
   u32 fixed;         // every block takes exactly maxbits bits
   u32 walk;          // decompress: offsets come from the batch walker
+  u64 start;         // bit of the first block; the stream's words below it (and the bits of
+  u64 hdr[3];        //   word start / 64 below start % 64) are the header hdr
 };
 
 // Blocks [first, first + count) of items[item].
@@ -177,9 +181,11 @@ struct BatchJob {
   void* field;
   u64* stream;
   u64 stream_words;
-  u64* index;
-  u64 end_bit;    // out: stream bits written / read
-  Status status;  // out
+  u64* index;          // block offsets relative to start_bit
+  u64 start_bit = 0;   // a zfp header of start_bit bits (<= 148) precedes the blocks:
+  u64 hdr[3] = {};     //   compress writes hdr there, decompress checks it
+  u64 end_bit;         // out: stream bits written / read
+  Status status;       // out
 };
 
 // Compress / decompress every job; each job's status and end_bit are set.

@@ -484,11 +484,11 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_bat
     const u64 blk = t.first + j;
     u64 o0, o1;
     if (it->fixed) {
-      o0 = blk * (u64)c.maxbits;
+      o0 = it->start + blk * (u64)c.maxbits;
       o1 = o0 + c.maxbits;
     } else {
-      o0 = offs[blk];
-      o1 = offs[blk + 1];
+      o0 = it->start + offs[blk];
+      o1 = it->start + offs[blk + 1];
     }
     Reader r;
     r.init(it->stream, it->stream_words, o0);
@@ -516,11 +516,11 @@ __global__ void __launch_bounds__(128, 8) k_parse_batch(BatchArgs a) {
     const u64 blk = t.first + j;
     u64 o0, o1;
     if (it->fixed) {
-      o0 = blk * (u64)c.maxbits;
+      o0 = it->start + blk * (u64)c.maxbits;
       o1 = o0 + c.maxbits;
     } else {
-      o0 = offs[blk];
-      o1 = offs[blk + 1];
+      o0 = it->start + offs[blk];
+      o1 = it->start + offs[blk + 1];
     }
     Reader r;
     r.init(it->stream, it->stream_words, o0);
@@ -572,7 +572,7 @@ __global__ void __launch_bounds__(64) k_walk_batch(BatchArgs a) {
   for (u64 blk = 0; blk < n; blk++) {
     off[blk] = rel;
     Reader r;
-    r.init(it->stream, it->stream_words, rel);
+    r.init(it->stream, it->stream_words, it->start + rel);
     if constexpr (S::N <= 64) {
       rel += block_length<T, S::N>(r, c);
     } else {

@@ -78,7 +78,8 @@ class ZfpBatchItem(C.Structure):
     """zfpb_batch_item (include/zfp_b200.h)."""
 
     _fields_ = [("desc", ZfpDesc), ("d_field", C.c_void_p), ("d_stream", C.c_void_p), ("stream_bytes", C.c_size_t),
-                ("d_block_offsets", C.c_void_p), ("result", C.c_size_t), ("status", C.c_int)]
+                ("d_block_offsets", C.c_void_p), ("header_mask", C.c_uint), ("result", C.c_size_t),
+                ("status", C.c_int)]
 
 
 class ZfpRequestDone(C.Structure):
@@ -395,13 +396,15 @@ def decompress_device(stream_t, nbytes: int, out, config: ZfpConfig, offsets=Non
     return n
 
 
-def batch_items(fields, configs, streams, nbytes=None, offsets=None):
+def batch_items(fields, configs, streams, nbytes=None, offsets=None, header_mask=0):
     """A ctypes array of zfpb_batch_item for torch CUDA tensors.
 
     fields[i] is a contiguous CUDA tensor (the input of a compress, the output
     of a decompress), streams[i] a CUDA tensor holding its stream, nbytes[i]
-    the stream size for a decompress (default: the stream tensor's size), and
-    offsets[i] an optional int64 CUDA tensor of nblocks + 1 block offsets.
+    the stream size for a decompress (default: the stream tensor's size),
+    offsets[i] an optional int64 CUDA tensor of nblocks + 1 block offsets, and
+    header_mask the ZFP_HEADER_* bits of the header each stream carries (an
+    int for all items, or one per item; 0 = none).
     """
     n = len(fields)
     items = (ZfpBatchItem * n)()
@@ -413,6 +416,7 @@ def batch_items(fields, configs, streams, nbytes=None, offsets=None):
         items[i].stream_bytes = nbytes[i] if nbytes is not None else st.numel() * st.element_size()
         o = offsets[i] if offsets is not None else None
         items[i].d_block_offsets = o.data_ptr() if o is not None else None
+        items[i].header_mask = header_mask[i] if isinstance(header_mask, (list, tuple)) else header_mask
     return items
 
 
