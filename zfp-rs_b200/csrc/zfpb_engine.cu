@@ -523,6 +523,7 @@ struct Buf {
 
 struct Workspace {
   Buf slots, lengths, offsets, partial, small, owner, planes, heads;
+  Buf spec_list, spec_fix, spec_seg;  // speculative walk
   u64* h_pinned = nullptr;  // two words for totals and flags
 };
 
@@ -730,6 +731,107 @@ static cudaError_t decode_blocks(Workspace& ws, const Call& call, const DecodeAr
   });
 }
 
+// Blocks per segment of the speculative walk (k_spec_walk).
+__global__ void k_spec_counts(SpecWalkArgs a) {
+  const u64 sg = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (sg < a.nseg) a.counts[sg] = a.fix_len[sg] + a.list_len[sg] - a.sync_j[sg];
+}
+
+// Each segment's true positions (its fix, then its list from where the true
+// walk joins it) to their places among the offsets; off[n] too when the
+// segments hold more than n positions.
+__global__ void k_spec_write(SpecWalkArgs a) {
+  const u64 sg = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (sg >= a.nseg) return;
+  const u64 lo = sg * a.seg_bits;
+  u64 idx = a.base[sg];
+  const u32* fix = a.fix + sg * a.cap;
+  const u32* list = a.list + sg * a.cap;
+  for (u32 i = 0; i < a.fix_len[sg] && idx <= a.n; i++) a.off[idx++] = lo + fix[i];
+  for (u32 j = a.sync_j[sg]; j < a.list_len[sg] && idx <= a.n; j++) a.off[idx++] = lo + list[j];
+}
+
+// Offsets (relative to start) of a variable-rate stream without an index by
+// the speculative parallel walk.  Sets *done when a.offsets holds them; else
+// (4D fields, short streams, a list overflow, no convergence) the caller
+// walks serially.  ZFPB_SERIAL_WALK=1 turns it off.
+static Status spec_walk(Workspace& ws, const Call& call, const DecodeArgs& a, cudaStream_t s, bool* done) {
+  *done = false;
+  const char* env = getenv("ZFPB_SERIAL_WALK");
+  if (call.dims > 3 || (env && env[0] == '1')) return OK;
+  const u64 n = call.f.nblocks;
+  const u64 end_bits = a.stream_len * 64 > a.start ? a.stream_len * 64 - a.start : 0;
+  if (n < 4096 || end_bits == 0) return OK;
+  const u64 avg = std::max<u64>(1, end_bits / n);
+  const u64 G = call.dims == 3 ? std::max<u64>(4096, n / 2048) : std::max<u64>(1024, n / 4096);
+  const u64 seg_bits = G * avg;
+  if (seg_bits >= (1ull << 31)) return OK;
+  const u64 nseg = (end_bits + seg_bits - 1) / seg_bits;
+  if (nseg < 4) return OK;
+  const u64 cap = G + G / 2 + 8192;
+  ZFPB_CHECK(ws.spec_list.ensure(nseg * cap * sizeof(u32)));
+  ZFPB_CHECK(ws.spec_fix.ensure(nseg * cap * sizeof(u32)));
+  ZFPB_CHECK(ws.spec_seg.ensure(nseg * (4 * sizeof(u32) + 4 * sizeof(u64)) + (nseg + 1) * sizeof(u64) + 64));
+  const u64 tiles = (nseg + SCAN_TILE - 1) / SCAN_TILE;
+  ZFPB_CHECK(ws.partial.ensure((tiles + 1) * sizeof(u64)));
+  SpecWalkArgs sa;
+  sa.stream = a.stream;
+  sa.stream_len = a.stream_len;
+  sa.start = a.start;
+  sa.c = a.c;
+  sa.nseg = nseg;
+  sa.seg_bits = seg_bits;
+  sa.end_bits = end_bits;
+  sa.cap = cap;
+  sa.list = (u32*)ws.spec_list.p;
+  sa.fix = (u32*)ws.spec_fix.p;
+  u64* w64 = (u64*)ws.spec_seg.p;
+  sa.exit_spec = w64;
+  sa.ex_in = w64 + nseg;
+  sa.ex_out = w64 + 2 * nseg;
+  sa.entry_used = w64 + 3 * nseg;
+  sa.base = w64 + 4 * nseg;  // nseg + 1
+  u32* w32 = (u32*)(w64 + 5 * nseg + 1);
+  sa.list_len = w32;
+  sa.fix_len = w32 + nseg;
+  sa.sync_j = w32 + 2 * nseg;
+  sa.counts = w32 + 3 * nseg;
+  sa.flags = (unsigned*)(w32 + 4 * nseg);
+  sa.off = a.offsets;
+  sa.n = n;
+  auto by_type = [&](auto launch) {
+    return for_type(call.type, [&](auto* tp) {
+      using T = std::remove_pointer_t<decltype(tp)>;
+      return launch((T*)nullptr);
+    });
+  };
+  ZFPB_CHECK(cudaMemsetAsync(sa.flags, 0, 2 * sizeof(unsigned), s));
+  ZFPB_CHECK(by_type([&](auto* tp) { return Launch<std::remove_pointer_t<decltype(tp)>>::spec_walk(call.dims, sa, s); }));
+  bool converged = false;
+  for (int pass = 0; pass < 64; pass++) {
+    ZFPB_CHECK(cudaMemsetAsync(sa.flags, 0, sizeof(unsigned), s));
+    ZFPB_CHECK(by_type([&](auto* tp) { return Launch<std::remove_pointer_t<decltype(tp)>>::spec_fix(call.dims, sa, s); }));
+    ZFPB_CHECK(cudaMemcpyAsync(ws.h_pinned + 2, sa.flags, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    ZFPB_CHECK(cudaStreamSynchronize(s));
+    const unsigned* hf = (const unsigned*)(ws.h_pinned + 2);
+    if (hf[1]) return OK;  // a list overflowed
+    std::swap(sa.ex_in, sa.ex_out);  // ex_in: the exits this pass found
+    if (!hf[0]) {
+      converged = true;
+      break;
+    }
+  }
+  if (!converged) return OK;
+  k_spec_counts<<<(unsigned)((nseg + 255) / 256), 256, 0, s>>>(sa);
+  ZFPB_CHECK(cudaGetLastError());
+  ZFPB_CHECK(scan_entries(sa.counts, nseg, sa.base, (u64*)ws.partial.p, s));
+  k_spec_write<<<(unsigned)((nseg + 63) / 64), 64, 0, s>>>(sa);
+  ZFPB_CHECK(cudaGetLastError());
+  ZFPB_CHECK(by_type([&](auto* tp) { return Launch<std::remove_pointer_t<decltype(tp)>>::spec_tail(call.dims, sa, s); }));
+  *done = true;
+  return OK;
+}
+
 Status decompress(const Call& call, const u64* d_in, u64 len, u64 start, void* d_field, u64* end_bit,
                   const u64* d_offsets, cudaStream_t s) {
   std::lock_guard<std::mutex> lock(g_mu);
@@ -794,17 +896,33 @@ Status decompress(const Call& call, const u64* d_in, u64 len, u64 start, void* d
     off = (u64*)ws.offsets.p;
     a.offsets = off;
     ZFPB_CHECK(cudaMemsetAsync(flags, 0, sizeof(unsigned), s));
+    bool spec = false;
     {
       KernelTimer t(K_WALK, s);
-      ZFPB_CHECK(for_type(call.type, [&](auto* tp) {
-        using T = std::remove_pointer_t<decltype(tp)>;
-        return Launch<T>::walk(call, a, s);
-      }));
+      const Status st = spec_walk(ws, call, a, s, &spec);
+      if (st != OK) return st;
     }
-    ZFPB_CHECK(decode_blocks(ws, call, a, true, s));
-    ZFPB_CHECK(cudaMemcpyAsync(ws.h_pinned, flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-    ZFPB_CHECK(cudaStreamSynchronize(s));
-    fl = *(unsigned*)ws.h_pinned;
+    if (spec) {
+      ZFPB_CHECK(decode_blocks(ws, call, a, true, s));
+      ZFPB_CHECK(cudaMemcpyAsync(ws.h_pinned, flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+      ZFPB_CHECK(cudaStreamSynchronize(s));
+      fl = *(unsigned*)ws.h_pinned;
+      if (fl & FLAG_BAD_INDEX) spec = false;  // not the serial walk's offsets: walk serially
+    }
+    if (!spec) {
+      ZFPB_CHECK(cudaMemsetAsync(flags, 0, sizeof(unsigned), s));
+      {
+        KernelTimer t(K_WALK, s);
+        ZFPB_CHECK(for_type(call.type, [&](auto* tp) {
+          using T = std::remove_pointer_t<decltype(tp)>;
+          return Launch<T>::walk(call, a, s);
+        }));
+      }
+      ZFPB_CHECK(decode_blocks(ws, call, a, true, s));
+      ZFPB_CHECK(cudaMemcpyAsync(ws.h_pinned, flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+      ZFPB_CHECK(cudaStreamSynchronize(s));
+      fl = *(unsigned*)ws.h_pinned;
+    }
   }
   ZFPB_CHECK(cudaMemcpyAsync(ws.h_pinned + 1, off + n, sizeof(u64), cudaMemcpyDeviceToHost, s));
   ZFPB_CHECK(cudaStreamSynchronize(s));

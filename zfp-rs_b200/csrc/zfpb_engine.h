@@ -50,6 +50,31 @@ struct EncodeVarArgs {
   u32* lengths;
 };
 
+// Speculative parallel walk of a variable-rate stream without an index (see
+// k_spec_walk).  Positions are bits relative to `start`; list and fix hold
+// positions relative to their segment's first bit.
+struct SpecWalkArgs {
+  const u64* stream;
+  u64 stream_len;  // words
+  u64 start;
+  CodecParams c;
+  u64 nseg, seg_bits, end_bits, cap;
+  u32* list;        // nseg * cap: the speculative walk's positions
+  u32* list_len;
+  u32* fix;         // nseg * cap: positions from the true entry up to the first listed one
+  u32* fix_len;
+  u32* sync_j;      // index in list where the true walk joins it (list_len: never)
+  u64* exit_spec;   // first position at or past the segment's end, speculative walk
+  u64* ex_in;       // each segment's exit as known before / after a fix pass
+  u64* ex_out;
+  u64* entry_used;  // entry the segment's fix was computed from (~0: none)
+  unsigned* flags;  // [0] an exit changed, [1] a list overflowed
+  u32* counts;      // blocks per segment
+  u64* base;        // their exclusive scan (nseg + 1)
+  u64* off;         // out: n + 1 block offsets
+  u64 n;
+};
+
 struct DecodeArgs {
   void* data;
   FieldGeom f;
@@ -220,6 +245,11 @@ template <class T> struct Launch {
   static cudaError_t decode_fixed(const Call& call, const DecodeArgs& a, cudaStream_t s);
   static cudaError_t decode_var(const Call& call, const DecodeArgs& a, cudaStream_t s);
   static cudaError_t walk(const Call& call, const DecodeArgs& a, cudaStream_t s);
+  // Passes of the speculative walk (dims 1-3): the walk, one fix pass, the
+  // blocks past the last segment.
+  static cudaError_t spec_walk(int dims, const SpecWalkArgs& a, cudaStream_t s);
+  static cudaError_t spec_fix(int dims, const SpecWalkArgs& a, cudaStream_t s);
+  static cudaError_t spec_tail(int dims, const SpecWalkArgs& a, cudaStream_t s);
   // Batches: one launch over `ntiles` tiles of (T, dims) arrays.
   static cudaError_t encode_batch(int dims, const BatchArgs& a, u32 ntiles, int threads, cudaStream_t s);
   static cudaError_t decode_batch(int dims, const BatchArgs& a, u32 ntiles, int threads, cudaStream_t s);

@@ -152,6 +152,35 @@ template <class T> cudaError_t Launch<T>::walk_batch(int dims, const BatchArgs& 
     default: return walk_batch_d<T, 4>(a, s);
   }
 }
+template <class T> cudaError_t Launch<T>::spec_walk(int dims, const SpecWalkArgs& a, cudaStream_t s) {
+  const unsigned g = (unsigned)((a.nseg + 63) / 64);
+  switch (dims) {
+    case 1: k_spec_walk<T, 1><<<g, 64, 0, s>>>(a); break;
+    case 2: k_spec_walk<T, 2><<<g, 64, 0, s>>>(a); break;
+    case 3: k_spec_walk<T, 3><<<g, 64, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+template <class T> cudaError_t Launch<T>::spec_fix(int dims, const SpecWalkArgs& a, cudaStream_t s) {
+  const unsigned g = (unsigned)((a.nseg + 63) / 64);
+  switch (dims) {
+    case 1: k_spec_fix<T, 1><<<g, 64, 0, s>>>(a); break;
+    case 2: k_spec_fix<T, 2><<<g, 64, 0, s>>>(a); break;
+    case 3: k_spec_fix<T, 3><<<g, 64, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+template <class T> cudaError_t Launch<T>::spec_tail(int dims, const SpecWalkArgs& a, cudaStream_t s) {
+  switch (dims) {
+    case 1: k_spec_tail<T, 1><<<1, 32, 0, s>>>(a); break;
+    case 2: k_spec_tail<T, 2><<<1, 32, 0, s>>>(a); break;
+    case 3: k_spec_tail<T, 3><<<1, 32, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
 template <class T> cudaError_t Launch<T>::walk(const Call& call, const DecodeArgs& a, cudaStream_t s) {
   ZFPB_DISPATCH(call, walk_d, a, s)
 }

@@ -431,6 +431,104 @@ __global__ void __launch_bounds__(32) k_walk(DecodeArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Speculative parallel walk.  A zfp stream has no block markers, but a walk
+// begun at a wrong bit reads some garbage blocks (most one or a few bits
+// long) and then lands on a true block start, after which it follows the
+// true walk (measured on smooth fields: a median of 60 steps for 1D, 950 for
+// 3D f64, never more than 7000).  So the stream is cut into segments, one
+// thread walks each from its first bit and lists the positions it visits
+// (k_spec_walk); a fix pass walks each segment again from the exit of the
+// one before until it meets a listed position, from which the list is the
+// true walk (k_spec_fix, repeated while an exit changes; segment 0 starts at
+// the true start, so the exits are exact after at most nseg passes, about
+// one in practice).  Counts, a scan and k_spec_write place the positions;
+// k_spec_tail walks any blocks past the last segment.  The decoder checks
+// every block's length against these offsets, and the caller walks serially
+// if that check or a list's capacity fails.
+// ---------------------------------------------------------------------------
+
+template <class T, int D> ZFPB_DEV u64 spec_len(const SpecWalkArgs& a, u64 x) {
+  Reader r;
+  r.init(a.stream, a.stream_len, a.start + x);
+  return block_length<T, KernelShape<T, D>::N>(r, a.c);
+}
+
+template <class T, int D> __global__ void __launch_bounds__(64) k_spec_walk(SpecWalkArgs a) {
+  const u64 sg = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (sg >= a.nseg) return;
+  const u64 lo = sg * a.seg_bits, hi = lo + a.seg_bits < a.end_bits ? lo + a.seg_bits : a.end_bits;
+  u32* list = a.list + sg * a.cap;
+  u64 x = lo, k = 0;
+  while (x < hi) {
+    if (k == a.cap) break;  // overflow: the caller walks serially
+    list[k++] = (u32)(x - lo);
+    x += spec_len<T, D>(a, x);
+  }
+  if (x < hi) atomicOr(a.flags + 1, 1u);
+  a.list_len[sg] = (u32)k;
+  a.exit_spec[sg] = x;
+  a.ex_in[sg] = x;
+  a.entry_used[sg] = sg == 0 ? 0ull : ~0ull;
+  a.fix_len[sg] = 0;
+  a.sync_j[sg] = 0;
+}
+
+template <class T, int D> __global__ void __launch_bounds__(64) k_spec_fix(SpecWalkArgs a) {
+  const u64 sg = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (sg >= a.nseg) return;
+  if (sg == 0) {
+    a.ex_out[0] = a.exit_spec[0];
+    return;
+  }
+  const u64 entry = a.ex_in[sg - 1];
+  if (entry == a.entry_used[sg]) {
+    a.ex_out[sg] = a.ex_in[sg];
+    return;
+  }
+  const u64 lo = sg * a.seg_bits, hi = lo + a.seg_bits < a.end_bits ? lo + a.seg_bits : a.end_bits;
+  const u32* list = a.list + sg * a.cap;
+  u32* fix = a.fix + sg * a.cap;
+  const u32 len = a.list_len[sg];
+  u64 x = entry, k = 0;
+  u32 j = 0;
+  bool joined = false;
+  while (x < hi) {
+    const u32 rx = (u32)(x - lo);
+    while (j < len && list[j] < rx) j++;
+    if (j < len && list[j] == rx) {
+      joined = true;
+      break;
+    }
+    if (k == a.cap) {  // overflow: the caller walks serially
+      atomicOr(a.flags + 1, 1u);
+      break;
+    }
+    fix[k++] = rx;
+    x += spec_len<T, D>(a, x);
+  }
+  a.fix_len[sg] = (u32)k;
+  a.sync_j[sg] = joined ? j : len;
+  const u64 ex = joined ? a.exit_spec[sg] : x;
+  a.ex_out[sg] = ex;
+  a.entry_used[sg] = entry;
+  if (ex != a.ex_in[sg]) atomicOr(a.flags, 1u);
+}
+
+// Every block of the walk that starts at or past the last segment's end (a
+// stream cut short, or blocks read past its last word), and off[n].
+template <class T, int D> __global__ void k_spec_tail(SpecWalkArgs a) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  u64 idx = a.base[a.nseg];
+  if (idx > a.n) return;  // off[n] was placed by k_spec_write
+  u64 x = a.ex_in[a.nseg - 1];
+  for (; idx < a.n; idx++) {
+    a.off[idx] = x;
+    x += spec_len<T, D>(a, x);
+  }
+  a.off[a.n] = x;
+}
+
+// ---------------------------------------------------------------------------
 // Batches: one CTA per tile (up to 128 consecutive blocks of one array, which
 // the CTA's threads take in turn), the arrays of one (type, dims) class in one
 // launch.  The per-block work is that of the
