@@ -761,9 +761,16 @@ static Status spec_walk(Workspace& ws, const Call& call, const DecodeArgs& a, cu
   if (call.dims > 3 || (env && env[0] == '1')) return OK;
   const u64 n = call.f.nblocks;
   const u64 end_bits = a.stream_len * 64 > a.start ? a.stream_len * 64 - a.start : 0;
-  if (n < 4096 || end_bits == 0) return OK;
+  if (n < 1024 || end_bits == 0) return OK;
+  // Segments of G blocks on average (one walker per warp) with a lead-in of
+  // L blocks, from a sweep on smooth fields (1D f32 2^22 values, 2D f32
+  // 1024^2, 3D f64 128^3 and 512^3): short segments and no lead-in for 1D,
+  // whose wrong-start walks join the true walk within a few hundred bits;
+  // 3D walks take up to a few thousand blocks to join, so its segments are
+  // longer and lead in by two segments.
   const u64 avg = std::max<u64>(1, end_bits / n);
-  const u64 G = call.dims == 3 ? std::max<u64>(4096, n / 2048) : std::max<u64>(1024, n / 4096);
+  const u64 G = call.dims == 3 ? std::max<u64>(512, n / 2048) : std::max<u64>(128, n / 8192);
+  const u64 L = call.dims == 1 ? 0 : call.dims == 2 ? 4 * G : 2 * G;
   const u64 seg_bits = G * avg;
   if (seg_bits >= (1ull << 31)) return OK;
   const u64 nseg = (end_bits + seg_bits - 1) / seg_bits;
@@ -783,6 +790,7 @@ static Status spec_walk(Workspace& ws, const Call& call, const DecodeArgs& a, cu
   sa.seg_bits = seg_bits;
   sa.end_bits = end_bits;
   sa.cap = cap;
+  sa.lead = L * avg;
   sa.list = (u32*)ws.spec_list.p;
   sa.fix = (u32*)ws.spec_fix.p;
   u64* w64 = (u64*)ws.spec_seg.p;

@@ -59,6 +59,7 @@ struct SpecWalkArgs {
   u64 start;
   CodecParams c;
   u64 nseg, seg_bits, end_bits, cap;
+  u64 lead;         // bits walked before a segment's first bit, unlisted
   u32* list;        // nseg * cap: the speculative walk's positions
   u32* list_len;
   u32* fix;         // nseg * cap: positions from the true entry up to the first listed one

@@ -152,22 +152,23 @@ template <class T> cudaError_t Launch<T>::walk_batch(int dims, const BatchArgs& 
     default: return walk_batch_d<T, 4>(a, s);
   }
 }
+// One walker per warp: a CTA of 32 threads per segment.
 template <class T> cudaError_t Launch<T>::spec_walk(int dims, const SpecWalkArgs& a, cudaStream_t s) {
-  const unsigned g = (unsigned)((a.nseg + 63) / 64);
+  const unsigned g = (unsigned)a.nseg;
   switch (dims) {
-    case 1: k_spec_walk<T, 1><<<g, 64, 0, s>>>(a); break;
-    case 2: k_spec_walk<T, 2><<<g, 64, 0, s>>>(a); break;
-    case 3: k_spec_walk<T, 3><<<g, 64, 0, s>>>(a); break;
+    case 1: k_spec_walk<T, 1><<<g, 32, 0, s>>>(a); break;
+    case 2: k_spec_walk<T, 2><<<g, 32, 0, s>>>(a); break;
+    case 3: k_spec_walk<T, 3><<<g, 32, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
 template <class T> cudaError_t Launch<T>::spec_fix(int dims, const SpecWalkArgs& a, cudaStream_t s) {
-  const unsigned g = (unsigned)((a.nseg + 63) / 64);
+  const unsigned g = (unsigned)a.nseg;
   switch (dims) {
-    case 1: k_spec_fix<T, 1><<<g, 64, 0, s>>>(a); break;
-    case 2: k_spec_fix<T, 2><<<g, 64, 0, s>>>(a); break;
-    case 3: k_spec_fix<T, 3><<<g, 64, 0, s>>>(a); break;
+    case 1: k_spec_fix<T, 1><<<g, 32, 0, s>>>(a); break;
+    case 2: k_spec_fix<T, 2><<<g, 32, 0, s>>>(a); break;
+    case 3: k_spec_fix<T, 3><<<g, 32, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

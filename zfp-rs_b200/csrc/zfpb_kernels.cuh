@@ -435,13 +435,16 @@ __global__ void __launch_bounds__(32) k_walk(DecodeArgs a) {
 // begun at a wrong bit reads some garbage blocks (most one or a few bits
 // long) and then lands on a true block start, after which it follows the
 // true walk (measured on smooth fields: a median of 60 steps for 1D, 950 for
-// 3D f64, never more than 7000).  So the stream is cut into segments, one
-// thread walks each from its first bit and lists the positions it visits
-// (k_spec_walk); a fix pass walks each segment again from the exit of the
-// one before until it meets a listed position, from which the list is the
-// true walk (k_spec_fix, repeated while an exit changes; segment 0 starts at
-// the true start, so the exits are exact after at most nseg passes, about
-// one in practice).  Counts, a scan and k_spec_write place the positions;
+// 3D f64, never more than 7000).  So the stream is cut into segments; for
+// each, one thread walks from `lead` bits before its first bit (so that it
+// has usually joined the true walk when it enters) and lists the positions
+// it visits inside the segment (k_spec_walk); a fix pass walks each segment
+// again from the exit of the one before until it meets a listed position,
+// from which the list is the true walk (k_spec_fix, repeated while an exit
+// changes; segment 0 starts at the true start, so the exits are exact after
+// at most nseg passes, one or two in practice).  Each walker has a warp to
+// itself: walkers sharing a warp diverge on every block and run several
+// times slower.  Counts, a scan and k_spec_write place the positions;
 // k_spec_tail walks any blocks past the last segment.  The decoder checks
 // every block's length against these offsets, and the caller walks serially
 // if that check or a list's capacity fails.
@@ -453,12 +456,14 @@ template <class T, int D> ZFPB_DEV u64 spec_len(const SpecWalkArgs& a, u64 x) {
   return block_length<T, KernelShape<T, D>::N>(r, a.c);
 }
 
-template <class T, int D> __global__ void __launch_bounds__(64) k_spec_walk(SpecWalkArgs a) {
-  const u64 sg = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (sg >= a.nseg) return;
+template <class T, int D> __global__ void __launch_bounds__(32) k_spec_walk(SpecWalkArgs a) {
+  const u64 sg = blockIdx.x;
+  if (threadIdx.x != 0 || sg >= a.nseg) return;
   const u64 lo = sg * a.seg_bits, hi = lo + a.seg_bits < a.end_bits ? lo + a.seg_bits : a.end_bits;
   u32* list = a.list + sg * a.cap;
-  u64 x = lo, k = 0;
+  u64 x = sg == 0 ? 0 : (lo > a.lead ? lo - a.lead : 0), k = 0;
+  for (u64 steps = 0; x < lo && steps < a.cap; steps++) x += spec_len<T, D>(a, x);  // lead-in, not listed
+  if (x < lo) x = lo;  // a lead-in that did not arrive: start at the segment
   while (x < hi) {
     if (k == a.cap) break;  // overflow: the caller walks serially
     list[k++] = (u32)(x - lo);
@@ -473,9 +478,9 @@ template <class T, int D> __global__ void __launch_bounds__(64) k_spec_walk(Spec
   a.sync_j[sg] = 0;
 }
 
-template <class T, int D> __global__ void __launch_bounds__(64) k_spec_fix(SpecWalkArgs a) {
-  const u64 sg = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (sg >= a.nseg) return;
+template <class T, int D> __global__ void __launch_bounds__(32) k_spec_fix(SpecWalkArgs a) {
+  const u64 sg = blockIdx.x;
+  if (threadIdx.x != 0 || sg >= a.nseg) return;
   if (sg == 0) {
     a.ex_out[0] = a.exit_spec[0];
     return;
