@@ -93,3 +93,38 @@ def test_truncated_stream_without_index():
         finally:
             os.environ.pop("ZFPB_SERIAL_WALK", None)
     assert errs == [2, 2]
+
+
+def test_batch_without_index_decodes_large_and_small_streams():
+    """A batch of streams without an index: large ones (decoded alone, by the
+    speculative walk) and small ones (walked in the batch) give what a decode
+    with the compressor's index gives; so do their headers."""
+    import torch
+
+    specs = [((1 << 18,), torch.float32, Z.ZfpConfig.fixed_accuracy(1e-5)),
+             ((3000,), torch.float64, Z.ZfpConfig.fixed_precision(24)),
+             ((260, 300), torch.float32, Z.ZfpConfig.fixed_precision(18)),
+             ((40, 30), torch.float64, Z.ZfpConfig.fixed_accuracy(1e-7)),
+             ((90, 100, 80), torch.float64, Z.ZfpConfig.fixed_accuracy(1e-6).with_rounding("first")),
+             ((9, 10, 11), torch.float32, Z.ZfpConfig.reversible())]
+    fields, cfgs, streams = [], [], []
+    for k, (shape, dt, c) in enumerate(specs):
+        x = field(shape, dt, seed=50 + k)
+        cap = Z.maximum_size(x.shape, Z._np_dtype(x.dtype), c)
+        st = torch.zeros((cap + 7) // 8, dtype=torch.int64, device="cuda")
+        fields.append(x)
+        cfgs.append(c)
+        streams.append(st)
+    items = Z.batch_items(fields, cfgs, streams, header_mask=7)
+    sizes = Z.compress_batch(items)
+    outs = [torch.full_like(x, 9) for x in fields]
+    used = Z.decompress_batch(Z.batch_items(outs, cfgs, streams, nbytes=sizes, header_mask=7))
+    assert used == sizes
+    for k, x in enumerate(fields):
+        nb = int(np.prod([(n + 3) // 4 for n in x.shape]))
+        off = torch.zeros(nb + 1, dtype=torch.int64, device="cuda")
+        st = torch.zeros_like(streams[k])
+        n = Z.compress_device(x, cfgs[k], out=st, offsets=off)
+        ref = torch.zeros_like(x)
+        Z.decompress_device(st, n, ref, cfgs[k], offsets=off)
+        assert torch.equal(outs[k].view(torch.uint8), ref.view(torch.uint8)), k

@@ -1680,8 +1680,12 @@ cudaError_t build_plan(BatchPlan& P, const BatchJob* jobs, const std::vector<u32
   return cudaSuccess;
 }
 
-// Split jobs into those the batch kernels take and those decoded alone
-// (fields whose strides alias); empty fields are done.
+// Split jobs into those the batch kernels take and those decoded alone:
+// fields whose strides alias, and large variable-rate streams without an
+// index, whose offsets the single-array decoder finds by the speculative
+// parallel walk (the batch walks one thread per stream, about 1.5-3.5 us a
+// block).  Empty fields are done.
+static constexpr u64 BATCH_WALK_MAX_BLOCKS = 8192;
 void classify(BatchJob* jobs, size_t n, bool compress, std::vector<u32>& batched, std::vector<u32>& single) {
   batched.clear();
   single.clear();
@@ -1691,7 +1695,8 @@ void classify(BatchJob* jobs, size_t n, bool compress, std::vector<u32>& batched
     J.end_bit = 0;
     const Call& c = J.call;
     if (c.f.nblocks == 0) continue;
-    if (!compress && strides_may_alias(c.f, c.dims)) single.push_back((u32)i);
+    const bool long_walk = !J.index && !fixed_size_blocks(c) && c.dims <= 3 && c.f.nblocks > BATCH_WALK_MAX_BLOCKS;
+    if (!compress && (strides_may_alias(c.f, c.dims) || long_walk)) single.push_back((u32)i);
     else batched.push_back((u32)i);
   }
 }
