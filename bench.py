@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-fixed", action="store_true", help="skip the fixed-rate float32 measurement")
+    ap.add_argument("--no-noindex", action="store_true",
+                    help="skip decoding the workload's stream without its block index")
     ap.add_argument("--batched-arrays", type=int, default=2000,
                     help="arrays in the batched workload (0 skips it)")
     ap.add_argument("--batched-max-elems", type=int, default=16_777_216,
@@ -363,6 +365,10 @@ def main():
     # Fixed-rate 8 float32, device resident.
     fr = None if args.no_fixed else fixed_rate_measure(Z, n, dev, args, peak)
 
+    # The same field's fixed-accuracy stream decoded without its block index
+    # (a stream from elsewhere): offsets from the speculative parallel walk.
+    ni = None if args.no_noindex else no_index_measure(Z, field, out, stream_buf, offsets, cfgs["accuracy_1e-6"], dev)
+
     # Batched workload (2,000 mixed arrays) against one call per array.
     del out, stream_buf
     torch.cuda.empty_cache()
@@ -389,6 +395,7 @@ def main():
             "gpu_launches": launches,
             "e2e": e2e,
             "fixed_rate_f32": fr,
+            "no_index_decode": ni,
             "batched": bt,
             "serving": sv,
             "clocks": clock_info,
@@ -705,6 +712,33 @@ def e2e_measure(Z, L, field, cfgs, cap, args, dev):
     return {"value": total / el / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d // args.steps,
             "d2h_bytes_per_step": d2h // args.steps, "ms_per_step": el * 1e3 / args.steps,
             "path": "zfp_compress/zfp_decompress (include/zfp.h) on pinned host buffers"}
+
+
+def no_index_measure(Z, field, out, stream_buf, offsets, cfg, dev, reps=3):
+    """Decompress of the field's stream with and without its block index
+    (best of `reps`, CUDA events around each call, the host synchronisations
+    of the call included): without one, zfpb_decompress_device finds the block
+    offsets by the speculative parallel walk before decoding."""
+    import torch
+
+    nb = Z.compress_device(field, cfg, out=stream_buf, offsets=offsets)
+
+    def timed(with_index):
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        Z.decompress_device(stream_buf, nb, out, cfg, offsets=offsets if with_index else None)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1)
+
+    timed(False)
+    with_index = min(timed(True) for _ in range(reps))
+    without = min(timed(False) for _ in range(reps))
+    return {"workload": f"{tuple(field.shape)} float64 fixed-accuracy 1e-6 stream, decompressed without its block index",
+            "blocks": int(offsets.numel() - 1), "stream_bytes": nb, "decode_with_index_ms": with_index,
+            "decode_without_index_ms": without,
+            "path": "zfpb_decompress_device without block offsets: speculative parallel walk, then the decoder"}
 
 
 def fixed_rate_measure(Z, n, dev, args, peak):
