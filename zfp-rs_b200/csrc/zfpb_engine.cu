@@ -523,7 +523,7 @@ struct Buf {
 
 struct Workspace {
   Buf slots, lengths, offsets, partial, small, owner, planes, heads;
-  Buf spec_list, spec_fix, spec_seg;  // speculative walk
+  Buf spec_list, spec_fix, spec_seg, spec_pieces;  // speculative walk
   u64* h_pinned = nullptr;  // two words for totals and flags
 };
 
@@ -731,30 +731,20 @@ static cudaError_t decode_blocks(Workspace& ws, const Call& call, const DecodeAr
   });
 }
 
-// Blocks per segment of the speculative walk (k_spec_walk).
-__global__ void k_spec_counts(SpecWalkArgs a) {
-  const u64 sg = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (sg < a.nseg) a.counts[sg] = a.fix_len[sg] + a.list_len[sg] - a.sync_j[sg];
-}
-
-// Each segment's true positions (its fix, then its list from where the true
-// walk joins it) to their places among the offsets; off[n] too when the
-// segments hold more than n positions.
-__global__ void k_spec_write(SpecWalkArgs a) {
-  const u64 sg = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (sg >= a.nseg) return;
-  const u64 lo = sg * a.seg_bits;
-  u64 idx = a.base[sg];
-  const u32* fix = a.fix + sg * a.cap;
-  const u32* list = a.list + sg * a.cap;
-  for (u32 i = 0; i < a.fix_len[sg] && idx <= a.n; i++) a.off[idx++] = lo + fix[i];
-  for (u32 j = a.sync_j[sg]; j < a.list_len[sg] && idx <= a.n; j++) a.off[idx++] = lo + list[j];
+// One CTA per piece of the speculative walk's chain: its positions (relative
+// to the segment they were listed in) to their places among the offsets.
+__global__ void k_spec_write(SpecWalkArgs a, const SpecPiece* pieces, u64* off, u64 n) {
+  const SpecPiece pc = pieces[blockIdx.x];
+  const u32* src = (pc.kind == 0 ? a.list : a.fix) + (u64)pc.seg * a.cap + pc.from;
+  const u64 lo = (u64)pc.seg * a.seg_bits;
+  for (u32 i = threadIdx.x; i < pc.count; i += blockDim.x)
+    if (pc.dst + i <= n) off[pc.dst + i] = lo + src[i];
 }
 
 // Offsets (relative to start) of a variable-rate stream without an index by
-// the speculative parallel walk.  Sets *done when a.offsets holds them; else
-// (4D fields, short streams, a list overflow, no convergence) the caller
-// walks serially.  ZFPB_SERIAL_WALK=1 turns it off.
+// the speculative parallel walk (k_spec_walk, k_spec_fix).  Sets *done when
+// a.offsets holds them; else (4D fields, short streams, a full list) the
+// caller walks serially.  ZFPB_SERIAL_WALK=1 turns it off.
 static Status spec_walk(Workspace& ws, const Call& call, const DecodeArgs& a, cudaStream_t s, bool* done) {
   *done = false;
   const char* env = getenv("ZFPB_SERIAL_WALK");
@@ -762,15 +752,15 @@ static Status spec_walk(Workspace& ws, const Call& call, const DecodeArgs& a, cu
   const u64 n = call.f.nblocks;
   const u64 end_bits = a.stream_len * 64 > a.start ? a.stream_len * 64 - a.start : 0;
   if (n < 1024 || end_bits == 0) return OK;
-  // Segments of G blocks on average (one walker per warp) with a lead-in of
-  // L blocks, from a sweep on smooth fields (1D f32 2^22 values, 2D f32
-  // 1024^2, 3D f64 128^3 and 512^3): short segments and no lead-in for 1D,
-  // whose wrong-start walks join the true walk within a few hundred bits;
-  // 3D walks take up to a few thousand blocks to join, so its segments are
-  // longer and lead in by two segments.
+  // Segments of G blocks on average, one walker per warp, about 4096 of them
+  // or fewer; a lead-in of L blocks before each.  A walk takes L + G steps
+  // plus its garbage start, and a fix about as many as the walks it meets
+  // took to join the true walk: a few hundred bits for 1D (no lead-in), up
+  // to a few thousand blocks for 2D and 3D (a lead-in of one segment; swept
+  // at 0, 1, 2 and 4 segments on 2D f32 1024^2 and 3D f64 128^3 and 512^3).
   const u64 avg = std::max<u64>(1, end_bits / n);
-  const u64 G = call.dims == 3 ? std::max<u64>(512, n / 2048) : std::max<u64>(128, n / 8192);
-  const u64 L = call.dims == 1 ? 0 : call.dims == 2 ? 4 * G : 2 * G;
+  const u64 G = std::max<u64>(call.dims == 1 ? 128 : call.dims == 2 ? 256 : 512, n / 4096);
+  const u64 L = call.dims == 1 ? 0 : G;
   const u64 seg_bits = G * avg;
   if (seg_bits >= (1ull << 31)) return OK;
   const u64 nseg = (end_bits + seg_bits - 1) / seg_bits;
@@ -778,9 +768,8 @@ static Status spec_walk(Workspace& ws, const Call& call, const DecodeArgs& a, cu
   const u64 cap = G + G / 2 + 8192;
   ZFPB_CHECK(ws.spec_list.ensure(nseg * cap * sizeof(u32)));
   ZFPB_CHECK(ws.spec_fix.ensure(nseg * cap * sizeof(u32)));
-  ZFPB_CHECK(ws.spec_seg.ensure(nseg * (4 * sizeof(u32) + 4 * sizeof(u64)) + (nseg + 1) * sizeof(u64) + 64));
-  const u64 tiles = (nseg + SCAN_TILE - 1) / SCAN_TILE;
-  ZFPB_CHECK(ws.partial.ensure((tiles + 1) * sizeof(u64)));
+  ZFPB_CHECK(ws.spec_seg.ensure(nseg * (2 * sizeof(u64) + 4 * sizeof(u32)) + 64));
+  ZFPB_CHECK(ws.spec_pieces.ensure(2 * nseg * sizeof(SpecPiece)));
   SpecWalkArgs sa;
   sa.stream = a.stream;
   sa.stream_len = a.stream_len;
@@ -795,47 +784,60 @@ static Status spec_walk(Workspace& ws, const Call& call, const DecodeArgs& a, cu
   sa.fix = (u32*)ws.spec_fix.p;
   u64* w64 = (u64*)ws.spec_seg.p;
   sa.exit_spec = w64;
-  sa.ex_in = w64 + nseg;
-  sa.ex_out = w64 + 2 * nseg;
-  sa.entry_used = w64 + 3 * nseg;
-  sa.base = w64 + 4 * nseg;  // nseg + 1
-  u32* w32 = (u32*)(w64 + 5 * nseg + 1);
+  sa.fix_exit = w64 + nseg;
+  u32* w32 = (u32*)(w64 + 2 * nseg);
   sa.list_len = w32;
   sa.fix_len = w32 + nseg;
-  sa.sync_j = w32 + 2 * nseg;
-  sa.counts = w32 + 3 * nseg;
-  sa.flags = (unsigned*)(w32 + 4 * nseg);
-  sa.off = a.offsets;
-  sa.n = n;
+  sa.sync_t = w32 + 2 * nseg;
+  sa.sync_j = w32 + 3 * nseg;
+  sa.flags = w32 + 4 * nseg;
   auto by_type = [&](auto launch) {
-    return for_type(call.type, [&](auto* tp) {
-      using T = std::remove_pointer_t<decltype(tp)>;
-      return launch((T*)nullptr);
-    });
+    return for_type(call.type, [&](auto* tp) { return launch(tp); });
   };
-  ZFPB_CHECK(cudaMemsetAsync(sa.flags, 0, 2 * sizeof(unsigned), s));
+  ZFPB_CHECK(cudaMemsetAsync(sa.flags, 0, sizeof(unsigned), s));
   ZFPB_CHECK(by_type([&](auto* tp) { return Launch<std::remove_pointer_t<decltype(tp)>>::spec_walk(call.dims, sa, s); }));
-  bool converged = false;
-  for (int pass = 0; pass < 64; pass++) {
-    ZFPB_CHECK(cudaMemsetAsync(sa.flags, 0, sizeof(unsigned), s));
-    ZFPB_CHECK(by_type([&](auto* tp) { return Launch<std::remove_pointer_t<decltype(tp)>>::spec_fix(call.dims, sa, s); }));
-    ZFPB_CHECK(cudaMemcpyAsync(ws.h_pinned + 2, sa.flags, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-    ZFPB_CHECK(cudaStreamSynchronize(s));
-    const unsigned* hf = (const unsigned*)(ws.h_pinned + 2);
-    if (hf[1]) return OK;  // a list overflowed
-    std::swap(sa.ex_in, sa.ex_out);  // ex_in: the exits this pass found
-    if (!hf[0]) {
-      converged = true;
+  ZFPB_CHECK(by_type([&](auto* tp) { return Launch<std::remove_pointer_t<decltype(tp)>>::spec_fix(call.dims, sa, s); }));
+  // The chain, on the host: segment 0's list; then for each segment entered
+  // at the exit of the list before it, its fix and the tail of the list the
+  // fix joined (whose exit leads into the next segment).
+  std::vector<u64> h64(2 * nseg);
+  std::vector<u32> h32(4 * nseg + 1);
+  ZFPB_CHECK(cudaMemcpyAsync(h64.data(), w64, 2 * nseg * sizeof(u64), cudaMemcpyDeviceToHost, s));
+  ZFPB_CHECK(cudaMemcpyAsync(h32.data(), w32, (4 * nseg + 1) * sizeof(u32), cudaMemcpyDeviceToHost, s));
+  ZFPB_CHECK(cudaStreamSynchronize(s));
+  if (h32[4 * nseg]) return OK;  // a list or fix overflowed
+  const u64* exit_spec = h64.data();
+  const u64* fix_exit = h64.data() + nseg;
+  const u32* list_len = h32.data();
+  const u32* fix_len = h32.data() + nseg;
+  const u32* sync_t = h32.data() + 2 * nseg;
+  const u32* sync_j = h32.data() + 3 * nseg;
+  std::vector<SpecPiece> pieces;
+  pieces.push_back({0, 0, 0, list_len[0], 0});
+  u64 total = list_len[0], last = exit_spec[0];
+  for (u64 sg = 1; sg < nseg && total <= n;) {
+    pieces.push_back({1, (u32)sg, 0, fix_len[sg], total});
+    total += fix_len[sg];
+    const u32 t = sync_t[sg];
+    if (t >= nseg) {
+      last = fix_exit[sg];
       break;
     }
+    pieces.push_back({0, t, sync_j[sg], list_len[t] - sync_j[sg], total});
+    total += list_len[t] - sync_j[sg];
+    last = exit_spec[t];
+    sg = (u64)t + 1;
   }
-  if (!converged) return OK;
-  k_spec_counts<<<(unsigned)((nseg + 255) / 256), 256, 0, s>>>(sa);
+  ZFPB_CHECK(cudaMemcpyAsync(ws.spec_pieces.p, pieces.data(), pieces.size() * sizeof(SpecPiece),
+                             cudaMemcpyHostToDevice, s));
+  k_spec_write<<<(unsigned)pieces.size(), 128, 0, s>>>(sa, (const SpecPiece*)ws.spec_pieces.p, a.offsets, n);
   ZFPB_CHECK(cudaGetLastError());
-  ZFPB_CHECK(scan_entries(sa.counts, nseg, sa.base, (u64*)ws.partial.p, s));
-  k_spec_write<<<(unsigned)((nseg + 63) / 64), 64, 0, s>>>(sa);
-  ZFPB_CHECK(cudaGetLastError());
-  ZFPB_CHECK(by_type([&](auto* tp) { return Launch<std::remove_pointer_t<decltype(tp)>>::spec_tail(call.dims, sa, s); }));
+  if (total <= n) {
+    ZFPB_CHECK(by_type([&](auto* tp) {
+      return Launch<std::remove_pointer_t<decltype(tp)>>::spec_tail(call.dims, sa, a.offsets, total, n, last, s);
+    }));
+  }
+  ZFPB_CHECK(cudaStreamSynchronize(s));  // the host's piece table is freed on return
   *done = true;
   return OK;
 }

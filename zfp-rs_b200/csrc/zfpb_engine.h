@@ -51,8 +51,9 @@ struct EncodeVarArgs {
 };
 
 // Speculative parallel walk of a variable-rate stream without an index (see
-// k_spec_walk).  Positions are bits relative to `start`; list and fix hold
-// positions relative to their segment's first bit.
+// k_spec_walk).  Positions are bits relative to `start`; segment s's list and
+// fix hold them relative to the segment's first bit (a fix may run on into
+// later segments; cap steps of at most a 4^4-double block stay below 2^32).
 struct SpecWalkArgs {
   const u64* stream;
   u64 stream_len;  // words
@@ -60,20 +61,22 @@ struct SpecWalkArgs {
   CodecParams c;
   u64 nseg, seg_bits, end_bits, cap;
   u64 lead;         // bits walked before a segment's first bit, unlisted
-  u32* list;        // nseg * cap: the speculative walk's positions
+  u32* list;        // nseg * cap: the speculative walk's positions in the segment
   u32* list_len;
-  u32* fix;         // nseg * cap: positions from the true entry up to the first listed one
-  u32* fix_len;
-  u32* sync_j;      // index in list where the true walk joins it (list_len: never)
   u64* exit_spec;   // first position at or past the segment's end, speculative walk
-  u64* ex_in;       // each segment's exit as known before / after a fix pass
-  u64* ex_out;
-  u64* entry_used;  // entry the segment's fix was computed from (~0: none)
-  unsigned* flags;  // [0] an exit changed, [1] a list overflowed
-  u32* counts;      // blocks per segment
-  u64* base;        // their exclusive scan (nseg + 1)
-  u64* off;         // out: n + 1 block offsets
-  u64 n;
+  u32* fix;         // nseg * cap: from the exit of segment s - 1 up to a listed position
+  u32* fix_len;
+  u32* sync_t;      // segment whose list the fix joined (nseg: none, the walk reached the end)
+  u32* sync_j;      // index in that list
+  u64* fix_exit;    // where a fix that joined no list stopped
+  unsigned* flags;  // [0] a list or fix overflowed
+};
+
+// One run of true block positions: `count` entries of segment `seg`'s list
+// (kind 0) or fix (kind 1) from index `from`, placed from off[dst].
+struct SpecPiece {
+  u32 kind, seg, from, count;
+  u64 dst;
 };
 
 struct DecodeArgs {
@@ -250,7 +253,7 @@ template <class T> struct Launch {
   // blocks past the last segment.
   static cudaError_t spec_walk(int dims, const SpecWalkArgs& a, cudaStream_t s);
   static cudaError_t spec_fix(int dims, const SpecWalkArgs& a, cudaStream_t s);
-  static cudaError_t spec_tail(int dims, const SpecWalkArgs& a, cudaStream_t s);
+  static cudaError_t spec_tail(int dims, const SpecWalkArgs& a, u64* off, u64 idx, u64 n, u64 x, cudaStream_t s);
   // Batches: one launch over `ntiles` tiles of (T, dims) arrays.
   static cudaError_t encode_batch(int dims, const BatchArgs& a, u32 ntiles, int threads, cudaStream_t s);
   static cudaError_t decode_batch(int dims, const BatchArgs& a, u32 ntiles, int threads, cudaStream_t s);

@@ -173,11 +173,12 @@ template <class T> cudaError_t Launch<T>::spec_fix(int dims, const SpecWalkArgs&
   }
   return cudaGetLastError();
 }
-template <class T> cudaError_t Launch<T>::spec_tail(int dims, const SpecWalkArgs& a, cudaStream_t s) {
+template <class T>
+cudaError_t Launch<T>::spec_tail(int dims, const SpecWalkArgs& a, u64* off, u64 idx, u64 n, u64 x, cudaStream_t s) {
   switch (dims) {
-    case 1: k_spec_tail<T, 1><<<1, 32, 0, s>>>(a); break;
-    case 2: k_spec_tail<T, 2><<<1, 32, 0, s>>>(a); break;
-    case 3: k_spec_tail<T, 3><<<1, 32, 0, s>>>(a); break;
+    case 1: k_spec_tail<T, 1><<<1, 32, 0, s>>>(a, off, idx, n, x); break;
+    case 2: k_spec_tail<T, 2><<<1, 32, 0, s>>>(a, off, idx, n, x); break;
+    case 3: k_spec_tail<T, 3><<<1, 32, 0, s>>>(a, off, idx, n, x); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

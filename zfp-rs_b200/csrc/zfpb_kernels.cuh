@@ -436,18 +436,17 @@ __global__ void __launch_bounds__(32) k_walk(DecodeArgs a) {
 // long) and then lands on a true block start, after which it follows the
 // true walk (measured on smooth fields: a median of 60 steps for 1D, 950 for
 // 3D f64, never more than 7000).  So the stream is cut into segments; for
-// each, one thread walks from `lead` bits before its first bit (so that it
-// has usually joined the true walk when it enters) and lists the positions
-// it visits inside the segment (k_spec_walk); a fix pass walks each segment
-// again from the exit of the one before until it meets a listed position,
-// from which the list is the true walk (k_spec_fix, repeated while an exit
-// changes; segment 0 starts at the true start, so the exits are exact after
-// at most nseg passes, one or two in practice).  Each walker has a warp to
-// itself: walkers sharing a warp diverge on every block and run several
-// times slower.  Counts, a scan and k_spec_write place the positions;
-// k_spec_tail walks any blocks past the last segment.  The decoder checks
-// every block's length against these offsets, and the caller walks serially
-// if that check or a list's capacity fails.
+// each, one thread walks from `lead` bits before its first bit and lists the
+// positions it visits inside the segment (k_spec_walk).  Then one fix pass
+// (k_spec_fix): for each segment s >= 1, a walk from the exit of segment
+// s - 1's list runs until it meets a position listed by s or by a later
+// segment, recording the positions before it.  Segment 0's list is exact (it
+// starts at the true start), so the true walk is segment 0's list, segment
+// 1's fix, the tail of the list it joined (whose exit is exact), the fix of
+// the segment after that one, and so on: a short chain the host follows
+// before k_spec_write places the pieces.  Each walker has a warp to itself:
+// walkers sharing a warp diverge on every block and run several times
+// slower.
 // ---------------------------------------------------------------------------
 
 template <class T, int D> ZFPB_DEV u64 spec_len(const SpecWalkArgs& a, u64 x) {
@@ -456,10 +455,15 @@ template <class T, int D> ZFPB_DEV u64 spec_len(const SpecWalkArgs& a, u64 x) {
   return block_length<T, KernelShape<T, D>::N>(r, a.c);
 }
 
+ZFPB_DEV u64 seg_hi(const SpecWalkArgs& a, u64 sg) {
+  const u64 hi = (sg + 1) * a.seg_bits;
+  return hi < a.end_bits ? hi : a.end_bits;
+}
+
 template <class T, int D> __global__ void __launch_bounds__(32) k_spec_walk(SpecWalkArgs a) {
   const u64 sg = blockIdx.x;
   if (threadIdx.x != 0 || sg >= a.nseg) return;
-  const u64 lo = sg * a.seg_bits, hi = lo + a.seg_bits < a.end_bits ? lo + a.seg_bits : a.end_bits;
+  const u64 lo = sg * a.seg_bits, hi = seg_hi(a, sg);
   u32* list = a.list + sg * a.cap;
   u64 x = sg == 0 ? 0 : (lo > a.lead ? lo - a.lead : 0), k = 0;
   for (u64 steps = 0; x < lo && steps < a.cap; steps++) x += spec_len<T, D>(a, x);  // lead-in, not listed
@@ -469,68 +473,62 @@ template <class T, int D> __global__ void __launch_bounds__(32) k_spec_walk(Spec
     list[k++] = (u32)(x - lo);
     x += spec_len<T, D>(a, x);
   }
-  if (x < hi) atomicOr(a.flags + 1, 1u);
+  if (x < hi) atomicOr(a.flags, 1u);
   a.list_len[sg] = (u32)k;
   a.exit_spec[sg] = x;
-  a.ex_in[sg] = x;
-  a.entry_used[sg] = sg == 0 ? 0ull : ~0ull;
-  a.fix_len[sg] = 0;
-  a.sync_j[sg] = 0;
 }
 
 template <class T, int D> __global__ void __launch_bounds__(32) k_spec_fix(SpecWalkArgs a) {
   const u64 sg = blockIdx.x;
   if (threadIdx.x != 0 || sg >= a.nseg) return;
-  if (sg == 0) {
-    a.ex_out[0] = a.exit_spec[0];
+  if (sg == 0) {  // exact: no fix, joins its own list at 0
+    a.fix_len[0] = 0;
+    a.sync_t[0] = 0;
+    a.sync_j[0] = 0;
+    a.fix_exit[0] = 0;
     return;
   }
-  const u64 entry = a.ex_in[sg - 1];
-  if (entry == a.entry_used[sg]) {
-    a.ex_out[sg] = a.ex_in[sg];
-    return;
-  }
-  const u64 lo = sg * a.seg_bits, hi = lo + a.seg_bits < a.end_bits ? lo + a.seg_bits : a.end_bits;
-  const u32* list = a.list + sg * a.cap;
+  const u64 lo = sg * a.seg_bits;
   u32* fix = a.fix + sg * a.cap;
-  const u32 len = a.list_len[sg];
-  u64 x = entry, k = 0;
+  u64 x = a.exit_spec[sg - 1], k = 0;
+  u64 t = x / a.seg_bits;  // the segment x lies in
   u32 j = 0;
   bool joined = false;
-  while (x < hi) {
-    const u32 rx = (u32)(x - lo);
+  while (x < a.end_bits) {
+    const u64 xt = x / a.seg_bits;
+    if (xt != t) {
+      t = xt;
+      j = 0;
+    }
+    const u32* list = a.list + t * a.cap;
+    const u32 len = a.list_len[t], rx = (u32)(x - t * a.seg_bits);
     while (j < len && list[j] < rx) j++;
     if (j < len && list[j] == rx) {
       joined = true;
       break;
     }
     if (k == a.cap) {  // overflow: the caller walks serially
-      atomicOr(a.flags + 1, 1u);
+      atomicOr(a.flags, 1u);
       break;
     }
-    fix[k++] = rx;
+    fix[k++] = (u32)(x - lo);
     x += spec_len<T, D>(a, x);
   }
   a.fix_len[sg] = (u32)k;
-  a.sync_j[sg] = joined ? j : len;
-  const u64 ex = joined ? a.exit_spec[sg] : x;
-  a.ex_out[sg] = ex;
-  a.entry_used[sg] = entry;
-  if (ex != a.ex_in[sg]) atomicOr(a.flags, 1u);
+  a.sync_t[sg] = joined ? (u32)t : (u32)a.nseg;
+  a.sync_j[sg] = joined ? j : 0u;
+  a.fix_exit[sg] = x;
 }
 
-// Every block of the walk that starts at or past the last segment's end (a
-// stream cut short, or blocks read past its last word), and off[n].
-template <class T, int D> __global__ void k_spec_tail(SpecWalkArgs a) {
+// Blocks idx .. n - 1 of the walk from x (past the segments: a stream cut
+// short, or blocks read past its last word), and off[n].
+template <class T, int D> __global__ void k_spec_tail(SpecWalkArgs a, u64* off, u64 idx, u64 n, u64 x) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  u64 idx = a.base[a.nseg];
-  if (idx > a.n) return;  // off[n] was placed by k_spec_write
-  u64 x = a.ex_in[a.nseg - 1];
-  for (; idx < a.n; idx++) {
-    a.off[idx] = x;
+  for (; idx < n; idx++) {
+    off[idx] = x;
     x += spec_len<T, D>(a, x);
   }
-  a.off[a.n] = x;
+  off[n] = x;
 }
 
 // ---------------------------------------------------------------------------
