@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--serve-rates", default="1000,5000",
                     help="serving: Poisson arrival rates (req/s), comma separated; empty skips")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="serving: length of each arrival stream")
+    ap.add_argument("--clock-csv", default="", help="also write the SM clock samples to this CSV file")
     ap.add_argument("--serve-small-rate", type=float, default=20000.0,
                     help="serving: rate of a stream of small requests (16 KB..1 MB); 0 skips")
     return ap.parse_args()
@@ -128,11 +129,11 @@ def smooth_f32(n, device, seed=0):
 class ClockSampler:
     """SM clocks and clock-event (throttle) reasons during the timed region,
     read through NVML every 2 ms from a thread (read-only queries); the
-    samples also go to a CSV file."""
+    samples also go to a CSV file when a path is given (--clock-csv)."""
 
     REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
-    def __init__(self, device_index: int, path: Path):
+    def __init__(self, device_index: int, path: Path | None):
         import threading
 
         self.path = path
@@ -177,13 +178,14 @@ class ClockSampler:
             return None
         self.stop_flag = True
         self.t.join(timeout=5)
-        try:
-            with open(self.path, "w") as f:
-                f.write("t_s,sm_mhz,reasons_mask\n")
-                for t, mhz, r in self.samples:
-                    f.write(f"{t:.4f},{mhz:.0f},{r:#x}\n")
-        except Exception:
-            pass
+        if self.path is not None:
+            try:
+                with open(self.path, "w") as f:
+                    f.write("t_s,sm_mhz,reasons_mask\n")
+                    for t, mhz, r in self.samples:
+                        f.write(f"{t:.4f},{mhz:.0f},{r:#x}\n")
+            except Exception:
+                pass
         if not self.samples:
             return None
         reasons = sorted(name for name, bit in self.REASONS.items() if any(r & bit for _, _, r in self.samples))
@@ -316,7 +318,7 @@ def main():
     torch.cuda.synchronize(dev)
     if pg is not None:
         pg.barrier()
-    clocks = ClockSampler(local, ROOT / "gpurun_out" / f"clocks_rank{rank}.csv") if rank == 0 else None
+    clocks = ClockSampler(local, Path(args.clock_csv) if args.clock_csv else None) if rank == 0 else None
     Z.timing_enable(True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)

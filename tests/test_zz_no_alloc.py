@@ -4,9 +4,11 @@ Some callers cannot let a library call cudaMalloc: an application that has
 reserved all device memory for its own pool, or a latency-critical loop that
 cannot take cudaMalloc's device-wide synchronization.  This entry point gives
 them the same stream as zfpb_compress_device, with its scratch taken from a
-fixed device array inside the library.  The test calls it through the C ABI
-twice in a row and checks each stream byte for byte against the existing
-entry point; it runs last (file name) and also alone in a fresh process.
+fixed device array inside the library.  The tests call it through the C ABI:
+first before any other entry point, checking that a call after the warm-up
+one leaves the device's free memory unchanged; then twice in a row per mode,
+checking each stream byte for byte against the existing entry point.  The
+file runs last (file name) and also passes alone in a fresh process.
 """
 
 import ctypes as C
@@ -46,6 +48,38 @@ def compress_both(x, cfg):
     assert na > 0 and nb == na, (na, nb, L.zfpb_last_error())
     assert torch.equal(a[: (na + 7) // 8], b[: (nb + 7) // 8])
     return na
+
+
+def test_noalloc_allocates_no_device_memory():
+    """The first library call of this file is the no-allocation entry point.
+
+    Its first call on a device loads the library's kernels (and with them
+    the module holding the fixed scratch array), which takes device memory
+    once.  After that warm-up call a second call must leave the device's
+    free memory unchanged; only then does the existing, allocating entry
+    point run, for the byte comparison."""
+    import torch
+
+    L = Z.lib()
+    x = field((24, 20, 28), 3, torch.float64)
+    cfg = Z.ZfpConfig.fixed_accuracy(1e-5)
+    desc = Z.desc_of(x.shape, np.float64, cfg)
+    cap = Z.maximum_size(x.shape, np.float64, cfg)
+    first = torch.zeros((cap + 7) // 8, dtype=torch.int64, device="cuda")
+    second = torch.zeros_like(first)
+    ref = torch.zeros_like(first)
+    cs = torch.cuda.current_stream().cuda_stream
+    n1 = L.zfpb_compress_device_noalloc(C.byref(desc), x.data_ptr(), first.data_ptr(), cap, cs)
+    assert n1 > 0, L.zfpb_last_error()
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    n2 = L.zfpb_compress_device_noalloc(C.byref(desc), x.data_ptr(), second.data_ptr(), cap, cs)
+    torch.cuda.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    assert n2 == n1 and free_after == free_before, (n1, n2, free_before, free_after)
+    nref = L.zfpb_compress_device(C.byref(desc), x.data_ptr(), ref.data_ptr(), cap, None, cs)
+    assert nref == n1
+    assert torch.equal(first, ref) and torch.equal(second, ref)
 
 
 @pytest.mark.parametrize("dtype_name", ["float32", "float64"])

@@ -507,7 +507,10 @@ template <class T, int D> __global__ void __launch_bounds__(32) k_spec_fix(SpecW
       joined = true;
       break;
     }
-    if (k == a.cap) {  // overflow: the caller walks serially
+    // Overflow (a full fix list, or a position past 2^32 bits from the
+    // segment's start, which the u32 entries cannot hold): the caller walks
+    // serially.
+    if (k == a.cap || x - lo > 0xffffffffull) {
       atomicOr(a.flags, 1u);
       break;
     }
