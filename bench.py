@@ -15,11 +15,18 @@ stream, and device->host copies of the stream and the decoded field, inside
 the timed region.
 
 Also reported (extra keys): fixed-rate 8 float32 512^3 compress/decompress
-GB/s and their roofline fractions.
+GB/s and their roofline fractions; the other workloads (the 64^3 float32
+plain array's latency, the 8192^2 float32 Gaussian random field at rates 4,
+12 and 24, the 2^28 int32 random walk and the 256^3 uniform int64 field in
+fixed-precision and reversible mode); the stream decoded without its block
+index; the batched 2,000-array workload and the serving loop.  All inputs
+come from tests/workloads.py (seeded, generated on the host).
 
---impl reference times the CPU restatement of zfp-rs (oracle/, the reference
-itself cannot be built here: no Rust toolchain) on the host cores, on bounded
-slabs of the same workload.
+--impl reference times the CPU restatement of zfp-rs (oracle/; the reference
+itself cannot be built here: no Rust toolchain) on all host cores: each step
+compresses and decompresses a 64-slice slab of the identical field in both
+modes with that step's rounding (chunked compress, reader/worker pipelined
+decode, as zfp-rs's Rayon path).
 """
 
 from __future__ import annotations
@@ -59,10 +66,12 @@ def parse():
                     help="arrays in the batched workload (0 skips it)")
     ap.add_argument("--batched-max-elems", type=int, default=16_777_216,
                     help="largest array of the batched workload, in elements")
-    ap.add_argument("--serve-rates", default="1000,5000",
+    ap.add_argument("--serve-rates", default="200,1000,5000",
                     help="serving: Poisson arrival rates (req/s), comma separated; empty skips")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="serving: length of each arrival stream")
     ap.add_argument("--clock-csv", default="", help="also write the SM clock samples to this CSV file")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other workloads (64^3 latency, 8192^2 rates, int32 walk, int64 field)")
     ap.add_argument("--serve-small-rate", type=float, default=20000.0,
                     help="serving: rate of a stream of small requests (16 KB..1 MB); 0 skips")
     return ap.parse_args()
@@ -76,54 +85,14 @@ def hbm_peak():
         return HBM_FALLBACK_GBS, "fallback"
 
 
-def make_field_np(n, nz, seed=0):
-    """The first nz z-slices of the workload field on the host (numpy).
-
-    Same recipe as make_field, drawn from numpy's generator (a slab for the
-    CPU baseline; values differ from the device field but follow the same
-    distribution)."""
-    rng = np.random.default_rng(seed)
-    x = np.arange(n, dtype=np.float64)
-    z = np.arange(nz, dtype=np.float64)
-    f = (np.sin(0.10 * x)[None, None, :] * np.cos(0.13 * x)[None, :, None] * np.sin(0.07 * z)[:, None, None])
-    f = (f + rng.normal(0, 1e-3, size=(nz, n, n))) * 1e3
-    nb, nbz = n // 4, nz // 4
-    zero = rng.random((nbz, nb, nb)) < 0.10
-    f.reshape(nbz, 4, nb, 4, nb, 4)[zero[:, None, :, None, :, None].repeat(4, 1).repeat(4, 3).repeat(4, 5)] = 0.0
-    spikes = rng.random(f.shape) < 0.01
-    k = int(spikes.sum())
-    f[spikes] = rng.choice([-1.0, 1.0], size=k) * 10.0 ** rng.uniform(-30, 30, size=k)
-    return f
+SLAB_Z = 64  # z-slices of the field in one reference-arm step (128 MiB of float64 at 512^2)
 
 
-def make_field(n, device, seed=0):
-    import torch
+def host_field(n, seed=0):
+    """The variable-rate workload's n^3 float64 field (tests/workloads.py)."""
+    from tests import workloads as W
 
-    g = torch.Generator(device=device)
-    g.manual_seed(seed)
-    x = torch.arange(n, device=device, dtype=torch.float64)
-    f = (torch.sin(0.10 * x)[None, None, :] * torch.cos(0.13 * x)[None, :, None] * torch.sin(0.07 * x)[:, None, None])
-    f = (f + 1e-3 * torch.randn((n, n, n), generator=g, device=device, dtype=torch.float64)) * 1e3
-    nb = n // 4
-    zero = torch.rand((nb, nb, nb), generator=g, device=device) < 0.10
-    zmask = zero.repeat_interleave(4, 0).repeat_interleave(4, 1).repeat_interleave(4, 2)
-    f[zmask] = 0.0
-    spikes = torch.rand((n, n, n), generator=g, device=device) < 0.01
-    k = int(spikes.sum())
-    sign = torch.where(torch.rand(k, generator=g, device=device) < 0.5, -1.0, 1.0).to(torch.float64)
-    mag = 10.0 ** (torch.rand(k, generator=g, device=device, dtype=torch.float64) * 60 - 30)
-    f[spikes] = sign * mag
-    return f
-
-
-def smooth_f32(n, device, seed=0):
-    import torch
-
-    g = torch.Generator(device=device)
-    g.manual_seed(seed)
-    x = torch.arange(n, device=device, dtype=torch.float32)
-    f = (torch.sin(0.10 * x)[None, None, :] * torch.cos(0.13 * x)[None, :, None] * torch.sin(0.07 * x)[:, None, None])
-    return f + 1e-3 * torch.randn((n, n, n), generator=g, device=device, dtype=torch.float32)
+    return W.spiky_f64(n, seed=seed)
 
 
 class ClockSampler:
@@ -219,30 +188,66 @@ def max_over_ranks(pg, value, device):
     return float(t.item())
 
 
-def cpu_baseline(n_side, threads, seconds_goal=15.0):
-    """The oracle (CPU restatement of zfp-rs) on slabs of the workload."""
+# The two modes of the variable-rate workload as expert parameters
+# (minbits, maxbits, maxprec, minexp): fixed_accuracy(1e-6) (min_exp =
+# frexp(1e-6).exponent - 1, zfp-rs config.rs:324-333) and fixed_precision(32).
+MODES = {"accuracy_1e-6": (1, 16658, 64, -20), "precision_32": (1, 16658, 32, -1074)}
+
+
+def cpu_steps(slab, threads, steps, first_step=0, gpu_streams=None):
+    """Steps of the oracle (the CPU restatement of zfp-rs) on `slab`: per step,
+    both modes with the step's rounding, compress (chunked over `threads`) then
+    decompress (reader/worker pipeline).  Returns (GB/s of uncompressed data,
+    seconds, {(mode, rounding index): stream bytes}); with `gpu_streams` (the
+    same keys: the GPU's stream of the same slab) also whether each matched."""
     from oracle import py_oracle as orc
 
-    slab_z = 32
-    field = make_field_np(n_side, slab_z)
-    cfgs = [orc.config(1, 16658, 64, -20, "first", False), orc.config(1, 16658, 32, -1074, "first", False)]
+    out = np.empty_like(slab)
+    streams = {}
     nbytes = 0
     t0 = time.perf_counter()
-    reps = 0
-    while True:
-        for cfg in cfgs:
-            stream, n = orc.compress(field, cfg, threads=threads)
-            out = np.zeros_like(field)
-            orc.decompress(stream, out, cfg, threads=threads)
-            nbytes += 2 * field.nbytes
-        reps += 1
-        el = time.perf_counter() - t0
-        if el >= seconds_goal or reps >= 8:
-            break
-    return {"value": nbytes / el / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
-            "sample": f"{n_side}x{n_side}x{slab_z} float64 slab x {reps} reps, fixed-accuracy 1e-6 + fixed-precision 32, "
-                      f"compress (chunked threads) + decompress (variable-rate: serial, as the restatement has no "
-                      f"reader/worker pipeline)"}
+    for i in range(first_step, first_step + steps):
+        ri = i % len(ROUNDINGS)
+        rnd, tight = ROUNDINGS[ri]
+        for name, params in MODES.items():
+            cfg = orc.config(*params, rnd, tight)
+            stream, n = orc.compress(slab, cfg, threads=threads)
+            assert n > 0 and orc.decompress(stream, out, cfg, threads=threads) == n
+            streams[(name, ri)] = stream
+            nbytes += 2 * slab.nbytes
+    el = time.perf_counter() - t0
+    same = None
+    if gpu_streams is not None:
+        same = {f"{k[0]}/{ROUNDINGS[k[1]][0]}{'+tight' if ROUNDINGS[k[1]][1] else ''}": gpu_streams.get(k) == v
+                for k, v in streams.items()}
+    return nbytes / el / 1e9, el, same
+
+
+def cpu_sample_text(n, threads, steps):
+    return (f"{n}x{n}x{SLAB_Z} float64 slab (the first {SLAB_Z} z-slices of the identical {n}^3 field) x {steps} "
+            f"steps, fixed-accuracy 1e-6 + fixed-precision 32, rounding First/Last x tight rotating per step; "
+            f"compress chunked over {threads} threads with bit concatenation (compress.rs:132-245), decompress "
+            f"through the reader/worker pipeline (decompress/pipeline.rs:193-229); C++ restatement of zfp-rs's "
+            f"CPU path (oracle/)")
+
+
+def cpu_baseline(field_np, threads, gpu_streams, steps=8):
+    """The CPU baseline beside the GPU arm: `steps` oracle steps on the slab,
+    and the byte comparison of its streams with the GPU's streams of the same
+    slab (one per mode and rounding)."""
+    slab = np.ascontiguousarray(field_np[:SLAB_Z])
+    v, el, same = cpu_steps(slab, threads, steps, gpu_streams=gpu_streams)
+    return {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": cpu_sample_text(field_np.shape[0], threads, steps), "seconds": el,
+            "gpu_stream_identical": same}
+
+
+def probe_cargo():
+    try:
+        r = subprocess.run(["cargo", "--version"], capture_output=True, text=True, timeout=20)
+        return r.stdout.strip() or f"exit {r.returncode}"
+    except Exception as e:  # absent from the image
+        return f"absent ({type(e).__name__})"
 
 
 def run_reference(args):
@@ -252,23 +257,22 @@ def run_reference(args):
             pg.destroy_process_group()
         return
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        pass
-    vals = []
-    samples = []
-    for _ in range(args.steps):
-        cb = cpu_baseline(args.size, threads, seconds_goal=4.0)
-        vals.append(cb["value"])
-        samples.append(cb)
-    v = float(np.mean(vals))
+    field = host_field(args.size)
+    slab = np.ascontiguousarray(field[:SLAB_Z])
+    del field
+    if args.warmup:
+        cpu_steps(slab, threads, args.warmup)
+    v, el, _ = cpu_steps(slab, threads, args.steps)
+    sample = cpu_sample_text(args.size, threads, args.steps)
     line = {"metric": "compress/decompress GB/s on 1 B200 (bit-exact); batched p50/p99 ms",
             "impl": "reference", "value": v, "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{args.size}^3 float64, fixed-accuracy 1e-6 + fixed-precision 32, "
-                                   "rounding First/Last x tight", "sampled": samples[0]["sample"]},
-            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
-                             "sample": samples[0]["sample"]},
+            "warmup": args.warmup, "ms_per_step": el * 1e3 / max(1, args.steps), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.size}^3 float64 smooth x1e3 + 10% zero blocks + 1% spikes; "
+                                   f"fixed-accuracy 1e-6 and fixed-precision 32, rounding First/Last x tight "
+                                   f"rotating per step", "sampled": sample},
+            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
+            "reference_toolchain": {"cargo": probe_cargo()},
             "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     if pg is not None:
@@ -290,7 +294,8 @@ def main():
     Z = zfpb.load()
     L = Z.lib()
     n = args.size
-    field = make_field(n, dev, seed=rank)
+    field_np = host_field(n, seed=rank)
+    field = torch.from_numpy(field_np).to(dev)
     nbytes = field.numel() * 8
     cfgs = {
         "accuracy_1e-6": Z.ZfpConfig.fixed_accuracy(1e-6),
@@ -371,9 +376,18 @@ def main():
     # (a stream from elsewhere): offsets from the speculative parallel walk.
     ni = None if args.no_noindex else no_index_measure(Z, field, out, stream_buf, offsets, cfgs["accuracy_1e-6"], dev)
 
-    # Batched workload (2,000 mixed arrays) against one call per array.
-    del out, stream_buf
+    # The GPU's streams of the CPU baseline's slab, for the byte comparison.
+    slab_streams = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        slab_streams = gpu_slab_streams(Z, field, cfgs, stream_buf)
+
+    # The other workloads: latency of the 64^3 plain array, 8192^2 float32 at
+    # fixed rates, the int32 walk and the int64 field.
+    del out, stream_buf, field
     torch.cuda.empty_cache()
+    oc = None if args.no_configs else configs_measure(Z, dev, args, peak)
+
+    # Batched workload (2,000 mixed arrays) against one call per array.
     bt = batched_measure(Z, dev, args) if args.batched_arrays > 0 else None
     rates = [float(r) for r in args.serve_rates.split(",") if r.strip()]
     sv = [serving_measure(Z, dev, args, r) for r in rates]
@@ -397,70 +411,110 @@ def main():
             "gpu_launches": launches,
             "e2e": e2e,
             "fixed_rate_f32": fr,
+            "other_workloads": oc,
             "no_index_decode": ni,
             "batched": bt,
             "serving": sv,
             "clocks": clock_info,
         }
         if ws == 1 and not args.no_cpu:
-            line["cpu_baseline"] = cpu_baseline(n, os.cpu_count() or 1)
+            line["cpu_baseline"] = cpu_baseline(field_np, os.cpu_count() or 1, slab_streams)
         print(json.dumps(line))
     if pg is not None:
         pg.destroy_process_group()
 
 
-def batched_workload(n_arrays, max_elems, dev, seed=0):
-    """2,000 arrays: 60% float32, 30% float64, 10% int32; 1D/2D/3D; element
-    counts log-uniform from 64 to max_elems, no side a multiple of 4; per-array
-    fixed-rate 2-32, fixed-precision 8-48 or fixed-accuracy 1e-2..1e-9 and a
-    random rounding; values sin(0.10x)cos(0.13y)sin(0.07z) + N(0, 1e-3) with
-    seed i (int32: scaled by 2^20).  Synthetic, seeded."""
+def gpu_slab_streams(Z, field, cfgs, buf):
+    """The GPU streams of the CPU baseline's slab (the first SLAB_Z z-slices of
+    the device field), one per mode and rounding, as bytes."""
     import torch
 
-    from tests import zfpb
+    slab = field[:SLAB_Z]
+    got = {}
+    for ri, (rnd, tight) in enumerate(ROUNDINGS):
+        for name, cfg in cfgs.items():
+            nb = Z.compress_device(slab, cfg.with_rounding(rnd, tight), out=buf)
+            got[(name, ri)] = buf.view(torch.uint8)[:nb].cpu().numpy().tobytes()
+    return got
 
-    Z = zfpb.load()
-    rng = np.random.default_rng(seed)
-    jobs = []
-    for i in range(n_arrays):
-        u = rng.random()
-        dtype = np.float32 if u < 0.6 else (np.float64 if u < 0.9 else np.int32)
-        dims = int(rng.integers(1, 4))
-        n = float(np.exp(rng.uniform(np.log(64), np.log(max_elems))))
-        base = n ** (1.0 / dims)
-        shape = []
-        for _ in range(dims):
-            side = max(1, int(round(base * rng.uniform(0.8, 1.25))))
-            if side % 4 == 0:
-                side += 1
-            shape.append(side)
-        g = torch.Generator(device=dev)
-        g.manual_seed(seed * 100003 + i)
-        freqs = [0.10, 0.13, 0.07]
-        funcs = [torch.sin, torch.cos, torch.sin]
-        f = torch.ones(shape, device=dev, dtype=torch.float64)
-        for ax in range(dims):  # x is the last (fastest) axis
-            c = torch.arange(shape[dims - 1 - ax], device=dev, dtype=torch.float64)
-            v = funcs[ax](freqs[ax] * c)
-            view = [1] * dims
-            view[dims - 1 - ax] = -1
-            f = f * v.view(view)
-        f = f + 1e-3 * torch.randn(shape, generator=g, device=dev, dtype=torch.float64)
-        if dtype == np.int32:
-            x = torch.round(f * 2 ** 20).to(torch.int32)
-        else:
-            x = f.to(torch.float32 if dtype == np.float32 else torch.float64)
-        kinds = 3 if dtype != np.int32 else 2
-        k = int(rng.integers(0, kinds))
-        if k == 0:
-            cfg = Z.ZfpConfig.fixed_rate(float(rng.integers(2, 33)), dtype, dims)
-        elif k == 1:
-            cfg = Z.ZfpConfig.fixed_precision(int(rng.integers(8, 49)))
-        else:
-            cfg = Z.ZfpConfig.fixed_accuracy(float(10.0 ** -rng.uniform(2, 9)))
-        cfg = cfg.with_rounding(["never", "first", "last"][int(rng.integers(0, 3))], bool(rng.integers(0, 2)))
-        jobs.append((x, cfg))
-    return jobs
+
+def timed_calls(fn, reps, dev):
+    """CUDA-event times (ms) of `reps` synchronous calls of fn on the current stream."""
+    import torch
+
+    cs = torch.cuda.current_stream(dev)
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(cs)
+        fn()
+        e1.record(cs)
+        torch.cuda.synchronize(dev)
+        ts.append(e0.elapsed_time(e1))
+    return ts
+
+
+def codec_leg(Z, x, cfg, reps, dev, peak, label):
+    """Compress and decompress of the device tensor x: per-call p50/p99 ms
+    (CUDA events around each call, host set-up included), GB/s of
+    uncompressed data at p50 and the algorithmic roofline fraction (field +
+    stream bytes over the p50 time)."""
+    import torch
+
+    cap = Z.maximum_size(x.shape, Z._np_dtype(x.dtype), cfg)
+    sb = torch.empty((cap + 7) // 8, dtype=torch.int64, device=dev)
+    nblk = int(np.prod([(m + 3) // 4 for m in x.shape]))
+    offs = torch.empty(nblk + 1, dtype=torch.int64, device=dev)
+    y = torch.empty_like(x)
+    nb = Z.compress_device(x, cfg, out=sb, offsets=offs)
+    for _ in range(3):
+        Z.compress_device(x, cfg, out=sb, offsets=offs)
+        Z.decompress_device(sb, nb, y, cfg, offsets=offs)
+    tc = timed_calls(lambda: Z.compress_device(x, cfg, out=sb, offsets=offs), reps, dev)
+    td = timed_calls(lambda: Z.decompress_device(sb, nb, y, cfg, offsets=offs), reps, dev)
+    fb = x.numel() * x.element_size()
+    pct = lambda v, q: float(np.percentile(v, q))
+    res = {"workload": label, "bytes": fb, "stream_bytes": nb, "reps": reps}
+    for key, ts in (("compress", tc), ("decompress", td)):
+        t = pct(ts, 50) / 1e3
+        res[f"{key}_ms_p50"] = pct(ts, 50)
+        res[f"{key}_ms_p99"] = pct(ts, 99)
+        res[f"{key}_gbs"] = fb / t / 1e9
+        res[f"{key}_roofline_frac"] = (fb + nb) / t / 1e9 / peak
+    if cfg.min_exp < -1074:
+        res["lossless"] = bool(torch.equal(x.view(torch.uint8).reshape(-1), y.view(torch.uint8).reshape(-1)))
+    return res
+
+
+def configs_measure(Z, dev, args, peak):
+    """The workloads other than the variable-rate field, device resident."""
+    import torch
+
+    from tests import workloads as W
+
+    reps = max(10, min(args.steps, 40))
+    out = {}
+    x = torch.from_numpy(W.smooth((64, 64, 64), seed=0)).to(dev)
+    out["plain_64cubed_f32_rate8"] = codec_leg(
+        Z, x, Z.ZfpConfig.fixed_rate(8, np.float32, 3), max(reps, 100), dev, peak,
+        "64^3 float32 smooth + N(0,1e-3), fixed-rate 8, rounding Never (launch-bound: latency)")
+    x = torch.from_numpy(W.grf_f32(8192)).to(dev)
+    for rate in (4, 12, 24):
+        out[f"grf_8192sq_f32_rate{rate}"] = codec_leg(
+            Z, x, Z.ZfpConfig.fixed_rate(rate, np.float32, 2), reps, dev, peak,
+            f"8192^2 float32 Gaussian random field (spectrum k^-3, seed 1), fixed-rate {rate}")
+    x = torch.from_numpy(W.random_walk_i32(1 << 28)).to(dev)
+    for name, cfg in (("precision20", Z.ZfpConfig.fixed_precision(20)), ("reversible", Z.ZfpConfig.reversible())):
+        out[f"walk_2p28_i32_{name}"] = codec_leg(
+            Z, x, cfg, reps, dev, peak, f"2^28 int32 random walk (steps U{{-100..100}}), {name}")
+    x = torch.from_numpy(W.uniform_i64((256, 256, 256))).to(dev)
+    for name, cfg in (("precision32", Z.ZfpConfig.fixed_precision(32)), ("reversible", Z.ZfpConfig.reversible())):
+        out[f"uniform_256cubed_i64_{name}"] = codec_leg(
+            Z, x, cfg, reps, dev, peak, f"256^3 int64 uniform in +-2^40, {name}")
+    del x
+    torch.cuda.empty_cache()
+    return out
 
 
 def batched_measure(Z, dev, args):
@@ -469,7 +523,10 @@ def batched_measure(Z, dev, args):
     zfpb_decompress_device call per array, same output checked bit for bit."""
     import torch
 
-    jobs = batched_workload(args.batched_arrays, args.batched_max_elems, dev)
+    from tests import workloads as W
+
+    specs = W.batched_specs(Z, args.batched_arrays, args.batched_max_elems)
+    jobs = [(W.batched_array(sp, i, dev), sp[2]) for i, sp in enumerate(specs)]
     fields = [x for x, _ in jobs]
     cfgs = [c for _, c in jobs]
     total = sum(x.numel() * x.element_size() for x in fields)
@@ -485,7 +542,7 @@ def batched_measure(Z, dev, args):
     Z.decompress_batch(ditems)
     Z.decompress_batch(ditems)
     cs = torch.cuda.current_stream(dev)
-    reps = max(5, args.steps)
+    reps = max(5, min(args.steps, 20))
 
     def timed(fn, n):
         ts = []
@@ -516,8 +573,8 @@ def batched_measure(Z, dev, args):
 
     per_array_compress()
     per_array_decompress()
-    sc = timed(per_array_compress, 2)
-    sd = timed(per_array_decompress, 2)
+    sc = timed(per_array_compress, reps)
+    sd = timed(per_array_decompress, reps)
     same = all(sizes[i] == single_sizes[i] and torch.equal(streams[i][: sizes[i] // 8], s2[i][: sizes[i] // 8])
                and torch.equal(outs[i].view(torch.uint8), o2[i].view(torch.uint8)) for i in range(len(jobs)))
     p = lambda v, q: float(np.percentile(v, q))
@@ -529,10 +586,11 @@ def batched_measure(Z, dev, args):
         "compress_ms_p50": p(bc, 50), "compress_ms_p99": p(bc, 99),
         "decompress_ms_p50": p(bd, 50), "decompress_ms_p99": p(bd, 99),
         "compress_gbs": total / (p(bc, 50) / 1e3) / 1e9, "decompress_gbs": total / (p(bd, 50) / 1e3) / 1e9,
-        "per_array_compress_ms": min(sc), "per_array_decompress_ms": min(sd),
-        "speedup_compress": min(sc) / p(bc, 50), "speedup_decompress": min(sd) / p(bd, 50),
+        "per_array_compress_ms_p50": p(sc, 50), "per_array_decompress_ms_p50": p(sd, 50),
+        "speedup_compress": p(sc, 50) / p(bc, 50), "speedup_decompress": p(sd, 50) / p(bd, 50),
         "identical_to_per_array": bool(same), "reps": reps,
-        "timing": "CUDA events on the calling stream around each whole call (host planning, graph launch, "
+        "timing": "p50 over the same number of repetitions for the batch and for one call per array; "
+                  "CUDA events on the calling stream around each whole call (host planning, graph launch, "
                   "per-array launches and synchronisations included)",
     }
     del streams, s2, outs, o2, fields, jobs
@@ -746,7 +804,9 @@ def no_index_measure(Z, field, out, stream_buf, offsets, cfg, dev, reps=3):
 def fixed_rate_measure(Z, n, dev, args, peak):
     import torch
 
-    x = smooth_f32(n, dev)
+    from tests import workloads as W
+
+    x = torch.from_numpy(W.smooth((n, n, n), seed=0)).to(dev)
     cfg = Z.ZfpConfig.fixed_rate(8, np.float32, 3)
     cap = Z.maximum_size(x.shape, np.float32, cfg)
     sb = torch.empty((cap + 7) // 8, dtype=torch.int64, device=dev)

@@ -10,9 +10,15 @@
 
 #include "zfp_oracle.h"
 
+#include <algorithm>
+#include <climits>
 #include <cmath>
+#include <condition_variable>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -750,31 +756,55 @@ template <class U> static void inv_round(U* d, int n, u32 m, u32 prec) {
   }
 }
 
-// bitplane.rs:626-667: returns bits read; fills u and *zero.
-template <class U, int N>
-static u32 decode_ints(Stream& s, u32 maxbits, u32 maxprec, int rounding, U* u, bool* zero_out) {
-  const u32 intprec = sizeof(U) * 8;
-  bool constrained = with_maxbits(maxbits, maxprec, N);
-  u32 budget = constrained ? maxbits : 0xffffffffu;
-  u32 kmin = intprec > maxprec ? intprec - maxprec : 0;
+// The stream half of decode_ints: the planes and the reader's state, which
+// finish_ints turns into coefficients (bitplane.rs:626-667; the pipeline's
+// read stage keeps exactly this per block, decode/staged.rs:216-267).
+template <class U, int N> struct IntsRead {
   Plane<N> planes[64];
-  for (u32 k = 0; k < intprec; k++) planes[k].clear();
+  PlaneResult pr;
+  bool constrained;
+  u32 kmin;
+  int rounding;
+};
+
+template <class U, int N>
+static u32 read_ints(Stream& s, u32 maxbits, u32 maxprec, int rounding, IntsRead<U, N>& st) {
+  const u32 intprec = sizeof(U) * 8;
+  st.constrained = with_maxbits(maxbits, maxprec, N);
+  u32 budget = st.constrained ? maxbits : 0xffffffffu;
+  st.kmin = intprec > maxprec ? intprec - maxprec : 0;
+  st.rounding = rounding;
+  for (u32 k = 0; k < intprec; k++) st.planes[k].clear();
   Reader r(s);
-  PlaneResult pr = decode_planes<N>(r, budget, kmin, intprec, planes);
+  st.pr = decode_planes<N>(r, budget, st.kmin, intprec, st.planes);
   r.sync();
-  bool zero = pr.low == intprec;
+  return st.pr.bits;
+}
+
+// The value half of decode_ints: fills u; returns the `zero` flag.
+template <class U, int N> static bool finish_ints(const IntsRead<U, N>& st, U* u) {
+  const u32 intprec = sizeof(U) * 8;
+  bool zero = st.pr.low == intprec;
   if (zero)
     for (int i = 0; i < N; i++) u[i] = 0;
   else
-    from_planes<U, N>(planes, u);
-  bool round = rounding == 2;
+    from_planes<U, N>(st.planes, u);
+  bool round = st.rounding == 2;
   if (round) {
-    u32 m = pr.m, prec = pr.prec;
-    if (!constrained) { m = 0; prec = intprec - (kmin - 1); }
+    u32 m = st.pr.m, prec = st.pr.prec;
+    if (!st.constrained) { m = 0; prec = intprec - (st.kmin - 1); }
     inv_round<U>(u, N, m, prec);
   }
-  *zero_out = zero && !round;
-  return pr.bits;
+  return zero && !round;
+}
+
+// bitplane.rs:626-667: returns bits read; fills u and *zero.
+template <class U, int N>
+static u32 decode_ints(Stream& s, u32 maxbits, u32 maxprec, int rounding, U* u, bool* zero_out) {
+  IntsRead<U, N> st;
+  u32 bits = read_ints<U, N>(s, maxbits, maxprec, rounding, st);
+  *zero_out = finish_ints<U, N>(st, u);
+  return bits;
 }
 
 // ---------------------------------------------------------------------------
@@ -1185,6 +1215,231 @@ static void dec_any(int type, Stream& s, const Plan& p, void* d, const Cfg& c, s
 }
 
 // ---------------------------------------------------------------------------
+// Staged block decoding: src/codec/decode/staged.rs.  read_block parses one
+// block's headers and bit planes and leaves the cursor after its padding;
+// reconstruct turns what it read into the block's values.  Together they do
+// what decode_block does, split so that the halves can run on different
+// threads.
+// ---------------------------------------------------------------------------
+
+enum { ST_ZERO, ST_FLOAT, ST_INT, ST_REV_INT, ST_REV_FLOAT, ST_REV_REINTERP };
+
+template <class T, int N> struct StagedBlock {
+  IntsRead<typename Tr<T>::U, N> ints;
+  int kind;
+  int32_t emax;
+};
+
+// staged.rs:216-267 (the grammar of decode/core.rs:97-237 and
+// decode/reversible.rs:46-228).
+template <class T, int N> static void read_block(Stream& s, const Cfg& c, StagedBlock<T, N>& b) {
+  typedef typename Tr<T>::U U;
+  const u32 dims = N == 4 ? 1 : N == 16 ? 2 : N == 64 ? 3 : 4;
+  const u32 PB = sizeof(U) == 4 ? 5 : 6;
+  b.emax = 0;
+  if (c.reversible()) {
+    if constexpr (Tr<T>::FLOAT) {
+      if (read_bits(s, 1) == 0) {
+        b.kind = ST_ZERO;
+        skip_to(s, 1, c.minbits);
+        return;
+      }
+      u32 bits = 2;
+      if (read_bits(s, 1)) {
+        b.kind = ST_REV_REINTERP;
+      } else {
+        b.kind = ST_REV_FLOAT;
+        b.emax = (int32_t)read_bits(s, Tr<T>::EBITS) - Tr<T>::EBIAS;
+        bits += Tr<T>::EBITS;
+      }
+      u32 mb = sat_sub(c.maxbits, bits);
+      u32 prec = (u32)read_bits(s, PB) + 1;
+      bits += PB + read_ints<U, N>(s, sat_sub(mb, PB), prec, 0, b.ints);
+      skip_to(s, bits, c.minbits);
+    } else {
+      b.kind = ST_REV_INT;
+      u32 prec = (u32)read_bits(s, PB) + 1;
+      u32 bits = PB + read_ints<U, N>(s, sat_sub(c.maxbits, PB), prec, 0, b.ints);
+      skip_to(s, bits, c.minbits);
+    }
+    return;
+  }
+  if constexpr (Tr<T>::FLOAT) {
+    if (read_bit(s)) {
+      const u32 hb = 1 + Tr<T>::EBITS;
+      b.kind = ST_FLOAT;
+      b.emax = (int32_t)read_bits(s, Tr<T>::EBITS) - Tr<T>::EBIAS;
+      u32 prec = precision_f(b.emax, c.maxprec, c.minexp, dims, c.tight);
+      u32 bits = read_ints<U, N>(s, sat_sub(c.maxbits, hb), prec, c.rounding, b.ints);
+      skip_to(s, bits, sat_sub(c.minbits, hb));
+    } else {
+      b.kind = ST_ZERO;
+      skip_to(s, 1, c.minbits);
+    }
+  } else {
+    b.kind = ST_INT;
+    u32 bits = read_ints<U, N>(s, c.maxbits, c.maxprec, c.rounding, b.ints);
+    skip_to(s, bits, c.minbits);
+  }
+}
+
+// staged.rs:52-144 (Scalar::reconstruct).
+template <class T, int N> static void reconstruct(const StagedBlock<T, N>& b, T* fb) {
+  typedef typename Tr<T>::I I;
+  typedef typename Tr<T>::U U;
+  if (b.kind == ST_ZERO) {
+    for (int i = 0; i < N; i++) fb[i] = 0;
+    return;
+  }
+  const unsigned char* perm = perm_of<N>();
+  U u[N];
+  I ib[N];
+  bool zero = finish_ints<U, N>(b.ints, u);
+  if (b.kind == ST_FLOAT || b.kind == ST_INT) {
+    for (int i = 0; i < N; i++) ib[i] = 0;
+    if (!zero) {
+      for (int i = 0; i < N; i++) ib[perm[i]] = uint2int(u[i]);
+      inv_xform<I, N>(ib);
+    }
+  } else {
+    for (int i = 0; i < N; i++) ib[perm[i]] = uint2int(u[i]);
+    rev_inv_xform<I, N>(ib);
+  }
+  if constexpr (Tr<T>::FLOAT) {
+    if (b.kind == ST_REV_REINTERP) {
+      const U tc = (U)(~(U)0) >> 1;
+      for (int i = 0; i < N; i++) fb[i] = ffrom(ib[i] < 0 ? (U)((U)ib[i] ^ tc) : (U)ib[i]);
+    } else {
+      inv_cast<T>(ib, fb, N, b.emax);
+    }
+  } else {
+    for (int i = 0; i < N; i++) fb[i] = ib[i];
+  }
+}
+
+// field_plan.rs:92-118: whether two index tuples may address one element.
+static bool strides_may_alias(const Plan& p) {
+  size_t st[4], dm[4];
+  int k = 0;
+  for (int d = 0; d < p.dims; d++)
+    if (p.n[d] >= 2) {
+      st[k] = (size_t)(p.s[d] < 0 ? -p.s[d] : p.s[d]);
+      dm[k] = p.n[d];
+      k++;
+    }
+  for (int i = 1; i < k; i++)  // sort by (stride, dim)
+    for (int j = i; j > 0 && (st[j] < st[j - 1] || (st[j] == st[j - 1] && dm[j] < dm[j - 1])); j--) {
+      std::swap(st[j], st[j - 1]);
+      std::swap(dm[j], dm[j - 1]);
+    }
+  size_t reach = 1;
+  for (int i = 0; i < k; i++) {
+    if (st[i] < reach) return true;
+    unsigned __int128 r = (unsigned __int128)st[i] * (dm[i] - 1) + reach;
+    reach = r > (unsigned __int128)SIZE_MAX ? SIZE_MAX : (size_t)r;
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// Variable-rate decode pipeline: src/decompress/pipeline.rs:15-229.  The
+// calling thread is the only reader of the stream: it reads batches of
+// blocks (64 KiB of staged blocks each) in stream order into a pool of at
+// most 16 buffers, and `threads - 1` workers reconstruct finished batches
+// and scatter them into disjoint blocks of the field.  Returns false,
+// having read nothing, where the reference falls back to the serial
+// decoder: 1-D fields, fewer than two threads, a field of one batch.
+// ---------------------------------------------------------------------------
+
+template <class T, int D>
+static bool decode_pipelined(Stream& s, const Plan& p, T* data, const Cfg& c, int threads) {
+  constexpr int N = 1 << (2 * D);
+  typedef StagedBlock<T, N> B;
+  if (D == 1 || threads < 2) return false;
+  const size_t batch_len = std::max<size_t>(1, 65536 / sizeof(B));
+  if (batch_len >= p.blocks) return false;
+  const size_t depth = std::min<size_t>(16, (p.blocks + batch_len - 1) / batch_len);
+  std::vector<std::vector<B>> bufs(depth, std::vector<B>(batch_len));
+  std::vector<size_t> first(depth), count(depth);
+  std::mutex mu;
+  std::condition_variable cv_free, cv_work;
+  std::deque<size_t> free_q, work_q;
+  bool done = false;
+  for (size_t i = 0; i < depth; i++) free_q.push_back(i);
+  auto worker = [&]() {
+    for (;;) {
+      size_t id;
+      {
+        std::unique_lock<std::mutex> l(mu);
+        cv_work.wait(l, [&] { return !work_q.empty() || done; });
+        if (work_q.empty()) return;
+        id = work_q.front();
+        work_q.pop_front();
+      }
+      for (size_t j = 0; j < count[id]; j++) {
+        ptrdiff_t off;
+        size_t len[4];
+        block_geometry(p, first[id] + j, &off, len);
+        T vals[N];
+        reconstruct<T, N>(bufs[id][j], vals);
+        scatter<T, D>(vals, data + off, p.s, len);
+      }
+      {
+        std::lock_guard<std::mutex> l(mu);
+        free_q.push_back(id);
+      }
+      cv_free.notify_one();
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads - 1; t++) pool.emplace_back(worker);
+  for (size_t start = 0; start < p.blocks;) {
+    size_t id;
+    {
+      std::unique_lock<std::mutex> l(mu);
+      cv_free.wait(l, [&] { return !free_q.empty(); });
+      id = free_q.front();
+      free_q.pop_front();
+    }
+    const size_t n = std::min(batch_len, p.blocks - start);
+    for (size_t j = 0; j < n; j++) read_block<T, N>(s, c, bufs[id][j]);
+    first[id] = start;
+    count[id] = n;
+    {
+      std::lock_guard<std::mutex> l(mu);
+      work_q.push_back(id);
+    }
+    cv_work.notify_one();
+    start += n;
+  }
+  {
+    std::lock_guard<std::mutex> l(mu);
+    done = true;
+  }
+  cv_work.notify_all();
+  for (auto& t : pool) t.join();
+  return true;
+}
+
+template <class T>
+static bool pipelined_any_dims(Stream& s, const Plan& p, void* d, const Cfg& c, int threads) {
+  switch (p.dims) {
+    case 2: return decode_pipelined<T, 2>(s, p, (T*)d, c, threads);
+    case 3: return decode_pipelined<T, 3>(s, p, (T*)d, c, threads);
+    case 4: return decode_pipelined<T, 4>(s, p, (T*)d, c, threads);
+    default: return false;
+  }
+}
+static bool pipelined_any(int type, Stream& s, const Plan& p, void* d, const Cfg& c, int threads) {
+  switch (type) {
+    case 1: return pipelined_any_dims<int32_t>(s, p, d, c, threads);
+    case 2: return pipelined_any_dims<int64_t>(s, p, d, c, threads);
+    case 3: return pipelined_any_dims<float>(s, p, d, c, threads);
+    default: return pipelined_any_dims<double>(s, p, d, c, threads);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Config inspectors: src/config.rs:469-686
 // ---------------------------------------------------------------------------
 
@@ -1347,7 +1602,10 @@ long long orc_decompress(void* sp, orc_field* f, const orc_config* cfg, int thre
   if (!make_plan(f, p) || f->data == nullptr) return -1;
   Cfg c = to_cfg(cfg);
   bool fixed = mode_of(cfg) == 2 && block_bits_of(cfg, f->type, p.dims) == cfg->maxbits;
-  if (threads > 1 && fixed && p.blocks >= 2) {
+  // decompress.rs:165-185: aliasing strides decode serially; fixed-rate
+  // streams in seek-parallel chunks, the others through the pipeline.
+  const bool shared = !strides_may_alias(p);
+  if (threads > 1 && shared && fixed && p.blocks >= 2) {
     u64 start_bit = rtell(s);
     u64 bpb = cfg->maxbits;
     u64 end = start_bit + (u64)p.blocks * bpb;
@@ -1375,7 +1633,8 @@ long long orc_decompress(void* sp, orc_field* f, const orc_config* cfg, int thre
     if (ov) s.overread = true;
   } else {
     reset_overread(s);
-    dec_any(f->type, s, p, f->data, c, 0, p.blocks);
+    if (!(threads > 1 && shared && mode_of(cfg) != 2 && pipelined_any(f->type, s, p, f->data, c, threads)))
+      dec_any(f->type, s, p, f->data, c, 0, p.blocks);
   }
   align(s);  // decompress.rs:66-74
   if (overread(s)) return -1;

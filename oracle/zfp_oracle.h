@@ -52,8 +52,10 @@ size_t orc_stream_size(void* s); /* bytes up to the cursor's word */
  * (compress.rs:132-245).  Returns the stream size in bytes, or -1 when the
  * buffer overflowed. */
 long long orc_compress(void* s, const orc_field* f, const orc_config* c, int threads);
-/* Whole-field decompression (decompress.rs:27-147); threads > 1 decodes
- * fixed-rate streams in seek-parallel chunks (decompress.rs:205-330).
+/* Whole-field decompression (decompress.rs:27-196).  threads > 1 and
+ * strides that cannot alias: fixed-rate streams decode in seek-parallel
+ * chunks (decompress.rs:205-330), other streams of 2-4 dimensions through the
+ * reader/worker pipeline (decompress/pipeline.rs:193-229); otherwise serial.
  * Returns bytes consumed, or -1 when the stream was truncated. */
 long long orc_decompress(void* s, orc_field* f, const orc_config* c, int threads);
 
