@@ -157,6 +157,23 @@ void zfpb_server_destroy(zfpb_server* s);
 void zfpb_timing_enable(int on);
 int zfpb_timing_read(double* ms, unsigned long long* counts, int n);
 
+/* Many whole blocks in one call: the batched form of the block-level calls
+ * of zfp_block.h (zfp-rs-ffi/src/block.rs:34-236, one block per call there).
+ * d_blocks holds `count` blocks of 4^dims values back to back (block i at
+ * element i * 4^dims, each laid out as zfp_encode_block_<type>_<dims> reads
+ * it); desc gives the type and the codec parameters (its sizes and strides
+ * are ignored).  zfpb_encode_blocks writes the stream that `count` calls of
+ * zfp_encode_block_<type>_<dims> on one stream followed by a flush write,
+ * from bit 0 of d_stream (capacity bytes), and returns its size in bytes
+ * (0 on failure); d_block_offsets (optional, count + 1 entries) receives
+ * each block's first bit.  zfpb_decode_blocks decodes such a stream back
+ * into d_blocks and returns the bytes consumed.  All buffers are device
+ * memory; the calls return once the work is done. */
+size_t zfpb_encode_blocks(const zfpb_desc* desc, uint dims, size_t count, const void* d_blocks, void* d_stream,
+                          size_t capacity, uint64_t* d_block_offsets, void* cuda_stream);
+size_t zfpb_decode_blocks(const zfpb_desc* desc, uint dims, size_t count, const void* d_stream,
+                          size_t stream_bytes, void* d_blocks, const uint64_t* d_block_offsets, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

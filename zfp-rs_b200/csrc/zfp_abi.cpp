@@ -19,6 +19,7 @@
 
 #include "../../include/zfp.h"
 #include "../../include/zfp_b200.h"
+#include "../../include/zfp_block.h"
 #include "zfpb_engine.h"
 #include "zfpb_serve.h"
 
@@ -1465,4 +1466,321 @@ extern "C" size_t zfpb_compress_device_noalloc(const zfpb_desc* d, const void* d
                                            (cudaStream_t)cuda_stream);
   if (st != zfpb::OK) return fail(st);
   return (size_t)((end + 63) / 64 * 8);
+}
+
+// ---------------------------------------------------------------------------
+// Block-level calls (zfp-rs-ffi/src/block.rs:25-776, codec/block/strided.rs:
+// 420-690): one 4^d block of a caller's array coded at the bit stream's
+// cursor, on the GPU.  The block is a field of one block (lengths 1..4 per
+// axis, the caller's element strides taken as given, 0 included), run
+// through the same engine as zfp_compress / zfp_decompress; the cursor is
+// left right after the block's bits, not flushed, so that calls append block
+// after block as the reference's do.  Returns the block's bits (after the
+// pad/skip to minbits), or 0 for a missing stream or pointer or an invalid
+// length.  Each call is one small GPU round trip: for many blocks
+// zfpb_encode_blocks / zfpb_decode_blocks code them in one call.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+DevBuf g_block_words;  // stream words of one block call (host bit streams)
+
+size_t block_call(zfp_stream* zs, zfp_type t, int dims, void* data, const ptrdiff_t* st, const size_t* len,
+                  bool encode) {
+  if (!zs || !zs->stream || !data) return 0;
+  for (int d = 0; d < dims; d++)
+    if (len[d] < 1 || len[d] > 4) return 0;  // strided.rs check_lengths
+  bitstream* bs = zs->stream;
+  const size_t es = type_size(t);
+  Plan p;
+  p.dims = dims;
+  p.nblocks = 1;
+  p.nelems = 1;
+  for (int d = 0; d < dims; d++) {
+    p.n[d] = len[d];
+    p.s[d] = st[d];
+    p.nelems *= len[d];
+    const ptrdiff_t ext = st[d] * (ptrdiff_t)(len[d] - 1);
+    if (ext < 0) p.imin += ext; else p.imax += ext;
+  }
+  p.span_bytes = (size_t)(p.imax - p.imin + 1) * es;
+  std::lock_guard<std::mutex> lock(g_abi_mu);
+  cudaStream_t s = lib_stream();
+  const bool host = !is_device_ptr(data);
+  char* begin = (char*)data + p.imin * (ptrdiff_t)es;
+  void* d_origin = data;
+  if (host) {
+    if (!g_field_stage.ensure(p.span_bytes)) return fail(zfpb::ERR_CUDA);
+    // Encode reads the span; decode keeps the gaps between strided elements.
+    if (cudaMemcpyAsync(g_field_stage.p, begin, p.span_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return fail(zfpb::ERR_CUDA);
+    d_origin = (char*)g_field_stage.p - p.imin * (ptrdiff_t)es;
+  }
+  zfpb::Call call;
+  call.type = t;
+  call.dims = dims;
+  call.f = geom_of(p, t, d_origin);
+  call.c = codec_of(zs);
+  const u64 bb = zfpb::block_bits(call.c, t, dims);
+  if (encode) {
+    const u64 start = bs_wtell(bs);
+    const u64 w0 = start / 64;
+    if (w0 > bs->len) {
+      bs->overflowed = true;
+      return fail(zfpb::ERR_OVERFLOW);
+    }
+    const u64 need = (start % 64 + bb + 63) / 64 + 1;
+    const u64 cap = bs->len - w0 < need ? bs->len - w0 : need;
+    u64* d_out = bs->words + w0;
+    if (!bs->device) {
+      if (!g_block_words.ensure(need * 8)) return fail(zfpb::ERR_CUDA);
+      d_out = (u64*)g_block_words.p;
+    }
+    const u64 init = bs->bits ? (bs->buffer & ((1ull << bs->bits) - 1)) : 0;
+    u64 end_rel = 0;
+    zfpb::Status stt = zfpb::compress(call, d_origin, d_out, cap, start % 64, init, &end_rel, nullptr, s);
+    if (stt == zfpb::ERR_OVERFLOW) {
+      bs->overflowed = true;
+      return fail(stt);
+    }
+    if (stt != zfpb::OK) return fail(stt);
+    const u64 end = w0 * 64 + end_rel;
+    const u64 wend = (end + 63) / 64;
+    if (!bs->device && wend > w0 &&
+        cudaMemcpyAsync(bs->words + w0, d_out, (wend - w0) * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+      return fail(zfpb::ERR_CUDA);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return fail(zfpb::ERR_CUDA);
+    // The cursor after the block, its partial word still buffered.
+    bs->word_pos = (size_t)(end / 64);
+    bs->bits = (u32)(end % 64);
+    bs->buffer = bs->bits ? get_word(bs, bs->word_pos) & ((1ull << bs->bits) - 1) : 0;
+    bs->index.valid = false;
+    return (size_t)(end - start);
+  }
+  const u64 start = bs_rtell(bs);
+  const u64 w0 = start / 64;
+  const u64 avail = bs->len > w0 ? bs->len - w0 : 0;
+  const u64 need = (start % 64 + bb + 63) / 64 + 2;
+  const u64 len_words = avail < need ? avail : need;
+  const u64* d_in = bs->words + w0;
+  if (!bs->device) {
+    if (!g_block_words.ensure((len_words + 1) * 8)) return fail(zfpb::ERR_CUDA);
+    if (len_words &&
+        cudaMemcpyAsync(g_block_words.p, bs->words + w0, len_words * 8, cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return fail(zfpb::ERR_CUDA);
+    d_in = (const u64*)g_block_words.p;
+  }
+  u64 end_rel = 0;
+  zfpb::Status stt = zfpb::decompress(call, d_in, len_words, start % 64, d_origin, &end_rel, nullptr, s);
+  if (stt != zfpb::OK && stt != zfpb::ERR_TRUNCATED) return fail(stt);
+  if (host && cudaMemcpyAsync(begin, g_field_stage.p, p.span_bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return fail(zfpb::ERR_CUDA);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return fail(zfpb::ERR_CUDA);
+  const u64 end = w0 * 64 + end_rel;
+  bs_seek_read(bs, end);
+  if (stt == zfpb::ERR_TRUNCATED) bs->overread = true;
+  return (size_t)(end - start);
+}
+
+// The contiguous layout of a whole block: x fastest, strides 1, 4, 16, 64.
+const ptrdiff_t kContig[4] = {1, 4, 16, 64};
+const size_t kWhole[4] = {4, 4, 4, 4};
+
+}  // namespace
+
+#define ZFPB_BLOCK_FNS(NAME, CT, ZT)                                                                              \
+  extern "C" size_t zfp_encode_block_##NAME##_1(zfp_stream* s, const CT* b) {                                   \
+    return block_call(s, ZT, 1, (void*)b, kContig, kWhole, true);                                                 \
+  }                                                                                                               \
+  extern "C" size_t zfp_encode_block_##NAME##_2(zfp_stream* s, const CT* b) {                                   \
+    return block_call(s, ZT, 2, (void*)b, kContig, kWhole, true);                                                 \
+  }                                                                                                               \
+  extern "C" size_t zfp_encode_block_##NAME##_3(zfp_stream* s, const CT* b) {                                   \
+    return block_call(s, ZT, 3, (void*)b, kContig, kWhole, true);                                                 \
+  }                                                                                                               \
+  extern "C" size_t zfp_encode_block_##NAME##_4(zfp_stream* s, const CT* b) {                                   \
+    return block_call(s, ZT, 4, (void*)b, kContig, kWhole, true);                                                 \
+  }                                                                                                               \
+  extern "C" size_t zfp_decode_block_##NAME##_1(zfp_stream* s, CT* b) {                                         \
+    return block_call(s, ZT, 1, b, kContig, kWhole, false);                                                       \
+  }                                                                                                               \
+  extern "C" size_t zfp_decode_block_##NAME##_2(zfp_stream* s, CT* b) {                                         \
+    return block_call(s, ZT, 2, b, kContig, kWhole, false);                                                       \
+  }                                                                                                               \
+  extern "C" size_t zfp_decode_block_##NAME##_3(zfp_stream* s, CT* b) {                                         \
+    return block_call(s, ZT, 3, b, kContig, kWhole, false);                                                       \
+  }                                                                                                               \
+  extern "C" size_t zfp_decode_block_##NAME##_4(zfp_stream* s, CT* b) {                                         \
+    return block_call(s, ZT, 4, b, kContig, kWhole, false);                                                       \
+  }                                                                                                               \
+  extern "C" size_t zfp_encode_block_strided_##NAME##_1(zfp_stream* s, const CT* b, ptrdiff_t sx) {             \
+    const ptrdiff_t st[4] = {sx, 0, 0, 0};                                                                        \
+    return block_call(s, ZT, 1, (void*)b, st, kWhole, true);                                                      \
+  }                                                                                                               \
+  extern "C" size_t zfp_encode_block_strided_##NAME##_2(zfp_stream* s, const CT* b, ptrdiff_t sx, ptrdiff_t sy) { \
+    const ptrdiff_t st[4] = {sx, sy, 0, 0};                                                                       \
+    return block_call(s, ZT, 2, (void*)b, st, kWhole, true);                                                      \
+  }                                                                                                               \
+  extern "C" size_t zfp_encode_block_strided_##NAME##_3(zfp_stream* s, const CT* b, ptrdiff_t sx, ptrdiff_t sy,  \
+                                                        ptrdiff_t sz) {                                           \
+    const ptrdiff_t st[4] = {sx, sy, sz, 0};                                                                      \
+    return block_call(s, ZT, 3, (void*)b, st, kWhole, true);                                                      \
+  }                                                                                                               \
+  extern "C" size_t zfp_encode_block_strided_##NAME##_4(zfp_stream* s, const CT* b, ptrdiff_t sx, ptrdiff_t sy,  \
+                                                        ptrdiff_t sz, ptrdiff_t sw) {                             \
+    const ptrdiff_t st[4] = {sx, sy, sz, sw};                                                                     \
+    return block_call(s, ZT, 4, (void*)b, st, kWhole, true);                                                      \
+  }                                                                                                               \
+  extern "C" size_t zfp_decode_block_strided_##NAME##_1(zfp_stream* s, CT* b, ptrdiff_t sx) {                   \
+    const ptrdiff_t st[4] = {sx, 0, 0, 0};                                                                        \
+    return block_call(s, ZT, 1, b, st, kWhole, false);                                                            \
+  }                                                                                                               \
+  extern "C" size_t zfp_decode_block_strided_##NAME##_2(zfp_stream* s, CT* b, ptrdiff_t sx, ptrdiff_t sy) {       \
+    const ptrdiff_t st[4] = {sx, sy, 0, 0};                                                                       \
+    return block_call(s, ZT, 2, b, st, kWhole, false);                                                            \
+  }                                                                                                               \
+  extern "C" size_t zfp_decode_block_strided_##NAME##_3(zfp_stream* s, CT* b, ptrdiff_t sx, ptrdiff_t sy,        \
+                                                        ptrdiff_t sz) {                                           \
+    const ptrdiff_t st[4] = {sx, sy, sz, 0};                                                                      \
+    return block_call(s, ZT, 3, b, st, kWhole, false);                                                            \
+  }                                                                                                               \
+  extern "C" size_t zfp_decode_block_strided_##NAME##_4(zfp_stream* s, CT* b, ptrdiff_t sx, ptrdiff_t sy,        \
+                                                        ptrdiff_t sz, ptrdiff_t sw) {                             \
+    const ptrdiff_t st[4] = {sx, sy, sz, sw};                                                                     \
+    return block_call(s, ZT, 4, b, st, kWhole, false);                                                            \
+  }                                                                                                               \
+  extern "C" size_t zfp_encode_partial_block_strided_##NAME##_1(zfp_stream* s, const CT* b, size_t nx,           \
+                                                                ptrdiff_t sx) {                                   \
+    const ptrdiff_t st[4] = {sx, 0, 0, 0};                                                                        \
+    const size_t n[4] = {nx, 0, 0, 0};                                                                            \
+    return block_call(s, ZT, 1, (void*)b, st, n, true);                                                           \
+  }                                                                                                               \
+  extern "C" size_t zfp_encode_partial_block_strided_##NAME##_2(zfp_stream* s, const CT* b, size_t nx,           \
+                                                                size_t ny, ptrdiff_t sx, ptrdiff_t sy) {          \
+    const ptrdiff_t st[4] = {sx, sy, 0, 0};                                                                       \
+    const size_t n[4] = {nx, ny, 0, 0};                                                                           \
+    return block_call(s, ZT, 2, (void*)b, st, n, true);                                                           \
+  }                                                                                                               \
+  extern "C" size_t zfp_encode_partial_block_strided_##NAME##_3(zfp_stream* s, const CT* b, size_t nx,           \
+                                                                size_t ny, size_t nz, ptrdiff_t sx, ptrdiff_t sy, \
+                                                                ptrdiff_t sz) {                                   \
+    const ptrdiff_t st[4] = {sx, sy, sz, 0};                                                                      \
+    const size_t n[4] = {nx, ny, nz, 0};                                                                          \
+    return block_call(s, ZT, 3, (void*)b, st, n, true);                                                           \
+  }                                                                                                               \
+  extern "C" size_t zfp_encode_partial_block_strided_##NAME##_4(zfp_stream* s, const CT* b, size_t nx,           \
+                                                                size_t ny, size_t nz, size_t nw, ptrdiff_t sx,    \
+                                                                ptrdiff_t sy, ptrdiff_t sz, ptrdiff_t sw) {       \
+    const ptrdiff_t st[4] = {sx, sy, sz, sw};                                                                     \
+    const size_t n[4] = {nx, ny, nz, nw};                                                                         \
+    return block_call(s, ZT, 4, (void*)b, st, n, true);                                                           \
+  }                                                                                                               \
+  extern "C" size_t zfp_decode_partial_block_strided_##NAME##_1(zfp_stream* s, CT* b, size_t nx, ptrdiff_t sx) { \
+    const ptrdiff_t st[4] = {sx, 0, 0, 0};                                                                        \
+    const size_t n[4] = {nx, 0, 0, 0};                                                                            \
+    return block_call(s, ZT, 1, b, st, n, false);                                                                 \
+  }                                                                                                               \
+  extern "C" size_t zfp_decode_partial_block_strided_##NAME##_2(zfp_stream* s, CT* b, size_t nx, size_t ny,      \
+                                                                ptrdiff_t sx, ptrdiff_t sy) {                     \
+    const ptrdiff_t st[4] = {sx, sy, 0, 0};                                                                       \
+    const size_t n[4] = {nx, ny, 0, 0};                                                                           \
+    return block_call(s, ZT, 2, b, st, n, false);                                                                 \
+  }                                                                                                               \
+  extern "C" size_t zfp_decode_partial_block_strided_##NAME##_3(zfp_stream* s, CT* b, size_t nx, size_t ny,      \
+                                                                size_t nz, ptrdiff_t sx, ptrdiff_t sy,            \
+                                                                ptrdiff_t sz) {                                   \
+    const ptrdiff_t st[4] = {sx, sy, sz, 0};                                                                      \
+    const size_t n[4] = {nx, ny, nz, 0};                                                                          \
+    return block_call(s, ZT, 3, b, st, n, false);                                                                 \
+  }                                                                                                               \
+  extern "C" size_t zfp_decode_partial_block_strided_##NAME##_4(zfp_stream* s, CT* b, size_t nx, size_t ny,      \
+                                                                size_t nz, size_t nw, ptrdiff_t sx, ptrdiff_t sy, \
+                                                                ptrdiff_t sz, ptrdiff_t sw) {                     \
+    const ptrdiff_t st[4] = {sx, sy, sz, sw};                                                                     \
+    const size_t n[4] = {nx, ny, nz, nw};                                                                         \
+    return block_call(s, ZT, 4, b, st, n, false);                                                                 \
+  }
+
+ZFPB_BLOCK_FNS(int32, int32_t, zfp_type_int32)
+ZFPB_BLOCK_FNS(int64, int64_t, zfp_type_int64)
+ZFPB_BLOCK_FNS(float, float, zfp_type_float)
+ZFPB_BLOCK_FNS(double, double, zfp_type_double)
+#undef ZFPB_BLOCK_FNS
+
+// ---------------------------------------------------------------------------
+// Integer promotion and demotion of one block of 4^dims values
+// (zfp-rs-ffi/src/promote.rs:11-59, src/codec/promote.rs): 8- and 16-bit
+// values to the int32 range the codec works in and back, clamped.  Plain
+// element maps on the caller's (host) arrays; dims outside 1..4 or a null
+// pointer do nothing.
+// ---------------------------------------------------------------------------
+
+namespace {
+template <class D, class S, class F> void map_block(D* out, const S* in, uint dims, F f) {
+  if (!out || !in || dims < 1 || dims > 4) return;
+  const size_t n = (size_t)1 << (2 * dims);
+  for (size_t i = 0; i < n; i++) out[i] = f(in[i]);
+}
+template <class T> T clamp_to(int32_t v, int32_t lo, int32_t hi) { return (T)(v < lo ? lo : v > hi ? hi : v); }
+}  // namespace
+
+extern "C" void zfp_promote_int8_to_int32(int32_t* o, const int8_t* i, uint dims) {
+  map_block(o, i, dims, [](int8_t x) { return (int32_t)((uint32_t)(int32_t)x << 23); });
+}
+extern "C" void zfp_promote_uint8_to_int32(int32_t* o, const uint8_t* i, uint dims) {
+  map_block(o, i, dims, [](uint8_t x) { return (int32_t)((uint32_t)((int32_t)x - 0x80) << 23); });
+}
+extern "C" void zfp_promote_int16_to_int32(int32_t* o, const int16_t* i, uint dims) {
+  map_block(o, i, dims, [](int16_t x) { return (int32_t)((uint32_t)(int32_t)x << 15); });
+}
+extern "C" void zfp_promote_uint16_to_int32(int32_t* o, const uint16_t* i, uint dims) {
+  map_block(o, i, dims, [](uint16_t x) { return (int32_t)((uint32_t)((int32_t)x - 0x8000) << 15); });
+}
+extern "C" void zfp_demote_int32_to_int8(int8_t* o, const int32_t* i, uint dims) {
+  map_block(o, i, dims, [](int32_t x) { return clamp_to<int8_t>(x >> 23, -0x80, 0x7f); });
+}
+extern "C" void zfp_demote_int32_to_uint8(uint8_t* o, const int32_t* i, uint dims) {
+  map_block(o, i, dims, [](int32_t x) { return clamp_to<uint8_t>((x >> 23) + 0x80, 0, 0xff); });
+}
+extern "C" void zfp_demote_int32_to_int16(int16_t* o, const int32_t* i, uint dims) {
+  map_block(o, i, dims, [](int32_t x) { return clamp_to<int16_t>(x >> 15, -0x8000, 0x7fff); });
+}
+extern "C" void zfp_demote_int32_to_uint16(uint16_t* o, const int32_t* i, uint dims) {
+  map_block(o, i, dims, [](int32_t x) { return clamp_to<uint16_t>((x >> 15) + 0x8000, 0, 0xffff); });
+}
+
+// ---------------------------------------------------------------------------
+// Many whole blocks in one GPU call (zfp_b200.h): `count` contiguous blocks
+// of 4^dims values (block i at element 4^dims * i, in the layout of
+// zfp_encode_block_*) are, to the codec, a field of 4 x .. x 4 x (4 * count)
+// values with natural strides, whose blocks come in exactly that order; the
+// stream is the one `count` calls of zfp_encode_block_<type>_<dims> on one
+// stream write, flushed to a word.
+// ---------------------------------------------------------------------------
+
+static bool blocks_desc(const zfpb_desc* d, uint dims, size_t count, zfpb_desc* out) {
+  if (!d || dims < 1 || dims > 4 || count == 0 || count > ((size_t)1 << 58)) return false;
+  *out = *d;
+  size_t* n[4] = {&out->nx, &out->ny, &out->nz, &out->nw};
+  ptrdiff_t* st[4] = {&out->sx, &out->sy, &out->sz, &out->sw};
+  for (uint i = 0; i < 4; i++) {
+    *n[i] = i < dims - 1 ? 4 : i == dims - 1 ? 4 * count : 0;
+    *st[i] = 0;
+  }
+  return true;
+}
+
+extern "C" size_t zfpb_encode_blocks(const zfpb_desc* d, uint dims, size_t count, const void* d_blocks,
+                                     void* d_stream, size_t capacity, uint64_t* d_block_offsets, void* cuda_stream) {
+  zfpb_desc f;
+  if (!blocks_desc(d, dims, count, &f)) return fail(zfpb::ERR_ARGS);
+  return zfpb_compress_device(&f, d_blocks, d_stream, capacity, d_block_offsets, cuda_stream);
+}
+
+extern "C" size_t zfpb_decode_blocks(const zfpb_desc* d, uint dims, size_t count, const void* d_stream,
+                                     size_t stream_bytes, void* d_blocks, const uint64_t* d_block_offsets,
+                                     void* cuda_stream) {
+  zfpb_desc f;
+  if (!blocks_desc(d, dims, count, &f)) return fail(zfpb::ERR_ARGS);
+  return zfpb_decompress_device(&f, d_stream, stream_bytes, d_blocks, d_block_offsets, cuda_stream);
 }

@@ -154,6 +154,31 @@ SIGNATURES = [
     ("zfpb_server_outstanding", _sz, [_vp]),
     ("zfpb_server_destroy", None, [_vp]),
 ]
+BLOCK_TYPES = ("int32", "int64", "float", "double")
+
+
+def _block_signatures():
+    """include/zfp_block.h (block-level calls, promotion) and the batched
+    block calls of include/zfp_b200.h."""
+    out = []
+    ss = C.c_ssize_t
+    for name in BLOCK_TYPES:
+        for d in (1, 2, 3, 4):
+            out += [(f"zfp_encode_block_{name}_{d}", _sz, [_S, _vp]),
+                    (f"zfp_decode_block_{name}_{d}", _sz, [_S, _vp]),
+                    (f"zfp_encode_block_strided_{name}_{d}", _sz, [_S, _vp] + [ss] * d),
+                    (f"zfp_decode_block_strided_{name}_{d}", _sz, [_S, _vp] + [ss] * d),
+                    (f"zfp_encode_partial_block_strided_{name}_{d}", _sz, [_S, _vp] + [_sz] * d + [ss] * d),
+                    (f"zfp_decode_partial_block_strided_{name}_{d}", _sz, [_S, _vp] + [_sz] * d + [ss] * d)]
+    for name in ("int8", "uint8", "int16", "uint16"):
+        out += [(f"zfp_promote_{name}_to_int32", None, [_vp, _vp, _u]),
+                (f"zfp_demote_int32_to_{name}", None, [_vp, _vp, _u])]
+    out += [("zfpb_encode_blocks", _sz, [C.POINTER(ZfpDesc), _u, _sz, _vp, _vp, _sz, _vp, _vp]),
+            ("zfpb_decode_blocks", _sz, [C.POINTER(ZfpDesc), _u, _sz, _vp, _sz, _vp, _vp, _vp])]
+    return out
+
+
+SIGNATURES += _block_signatures()
 DATA_SYMBOLS = ["stream_word_bits", "zfp_codec_version", "zfp_library_version"]
 
 _lib = None
