@@ -1082,6 +1082,10 @@ ZFPB_DEV u32 ctz64(u64 x) { return x ? (u32)__ffsll((long long)x) - 1 : 64u; }
 struct PlaneResult {
   u32 bits, m, prec;
   int low, high;  // stored planes are [low, high]; low = intprec if none
+  // With a verbatim tail left in the stream (decode_planes_sync's TAIL):
+  // whether one was found, and the stream bit where it starts.
+  u32 tail = 0;
+  u64 tail_pos = 0;
 };
 
 // decode_planes (bitplane.rs:675-790): planes go to the plane store.
@@ -1373,11 +1377,22 @@ ZFPB_DEV void group_tests(u64 t0, u64 t1, u32 n, u32 a, u32& end, u32& n_new, u3
 // Same contract and results as decode_planes, for N <= 64.  With QW != 0
 // (4-value blocks of QW * 16 planes) the planes go to the nibble string q
 // instead of the plane store.
-template <int N, int QW = 0>
+//
+// With TAIL (64-value blocks), the planes read once every coefficient is
+// significant are not stored: they are the stream's next bits verbatim, a
+// plane per 64 bits (the last one cut at the budget), so the reader's state
+// after them follows arithmetically and the value half reads them from the
+// stream itself.  The planes stored are then those down to the last group-test
+// plane (`low`), the tail planes run from low - 1 down, and the result's m
+// and prec are those of the full read.
+template <int N, int QW = 0, bool TAIL = false>
 ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 intprec, PlaneStore ps,
                                         u64* q = nullptr) {
   static_assert(N <= 64, "one plane word per plane");
   static_assert(QW == 0 || N == 4, "nibble planes are for 4-value blocks");
+  static_assert(!TAIL || N == 64, "verbatim tails are for 64-value blocks");
+  u32 tail = 0;
+  u64 tail_pos = 0;
   constexpr u32 size = N;
   // Plane kk (its bits and, with `np` planes, the ones below it) to the store.
   auto put = [&](u32 kk, u64 x, u32 np) {
@@ -1397,6 +1412,33 @@ ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 in
   bool done = false;
   while (bits != 0) {
     if (N <= 16 && n == size) break;  // verbatim tail below
+    if constexpr (TAIL) {
+      if (n == size) {
+        // Each remaining iteration reads a whole plane while more than a
+        // plane of budget is left (m = 0), then the rest of the budget as a
+        // last plane (m = those bits); or, out of planes, ends with m = 0
+        // and k one below kmin.
+        tail_pos = r.pos();
+        const u32 full_left = (bits - 1) / size, planes_left = k - kmin;
+        const u32 f = full_left < planes_left ? full_left : planes_left;
+        u32 used = f * size;
+        k -= f;
+        bits -= used;
+        if (k <= kmin) {
+          m = 0;
+          k = k - 1;
+        } else {
+          k = k - 1;
+          m = bits;
+          used += bits;
+          bits = 0;
+        }
+        tail = used != 0;
+        r.advance_far(used);
+        done = true;
+        break;
+      }
+    }
     m = 0;
     if (k <= kmin) {
       k = k - 1;
@@ -1538,6 +1580,8 @@ ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 in
   res.prec = intprec - k;
   res.low = low;
   res.high = high;
+  res.tail = tail;
+  res.tail_pos = tail_pos;
   return res;
 }
 
@@ -1953,25 +1997,41 @@ struct BlockHead {
   u32 m, prec;    // inverse-rounding arguments
   bool round;     // ROUND_LAST
   bool z;         // no plane stored
+  // The planes below `low` left in the stream (64-value blocks): a verbatim
+  // run from bit tail_pos, one plane per 64 bits from plane low - 1 down,
+  // the last one cut to m bits when m != 0 (see decode_planes_sync).
+  bool tail;
+  u64 tail_pos;
 
-  // kind 3 bits, emax + 2048 12 bits, low 9, high + 1 9, m 9, prec 8, round, z.
-  ZFPB_DEV u64 pack() const {
-    return (u64)kind | ((u64)(u32)(emax + 2048) & 0xfff) << 3 | (u64)((u32)low & 0x1ff) << 15 |
-           (u64)((u32)(high + 1) & 0x1ff) << 24 | (u64)(m & 0x1ff) << 33 | (u64)(prec & 0xff) << 42 |
-           (u64)round << 50 | (u64)z << 51;
+  // For 64-value blocks, in one word with the tail's offset from the block's
+  // first bit (`start`): kind 3 bits, emax + 2048 12, low 7, high + 1 7, m 7,
+  // prec 7, round, z, tail, tail offset 15 (a block has at most 16658 bits).
+  ZFPB_DEV u64 pack(u64 start) const {
+    const u64 toff = tail ? tail_pos - start : 0;
+    return (u64)kind | ((u64)(u32)(emax + 2048) & 0xfff) << 3 | (u64)((u32)low & 0x7f) << 15 |
+           (u64)((u32)(high + 1) & 0x7f) << 22 | (u64)(m & 0x7f) << 29 | (u64)(prec & 0x7f) << 36 |
+           (u64)round << 43 | (u64)z << 44 | (u64)tail << 45 | (toff & 0x7fff) << 46;
   }
-  ZFPB_DEV static BlockHead unpack(u64 v) {
+  ZFPB_DEV static BlockHead unpack(u64 v, u64 start) {
     BlockHead h;
     h.kind = (u32)(v & 7);
     h.emax = (int)((v >> 3) & 0xfff) - 2048;
-    h.low = (int)((v >> 15) & 0x1ff);
-    h.high = (int)((v >> 24) & 0x1ff) - 1;
-    h.m = (u32)((v >> 33) & 0x1ff);
-    h.prec = (u32)((v >> 42) & 0xff);
-    h.round = (v >> 50) & 1;
-    h.z = (v >> 51) & 1;
+    h.low = (int)((v >> 15) & 0x7f);
+    h.high = (int)((v >> 22) & 0x7f) - 1;
+    h.m = (u32)((v >> 29) & 0x7f);
+    h.prec = (u32)((v >> 36) & 0x7f);
+    h.round = (v >> 43) & 1;
+    h.z = (v >> 44) & 1;
+    h.tail = (v >> 45) & 1;
+    h.tail_pos = start + ((v >> 46) & 0x7fff);
     return h;
   }
+};
+
+// Where the value half finds a block's verbatim tail: the stream (len words).
+struct TailSrc {
+  const u64* stream;
+  u64 len;
 };
 
 // decode_ints, stream half: read the planes into ps; returns bits read.
@@ -1982,11 +2042,14 @@ ZFPB_DEV u32 parse_ints(Reader& r, u32 maxbits, u32 maxprec, int rounding, Plane
   const u32 budget = constrained ? maxbits : 0xffffffffu;
   const u32 kmin = intprec > maxprec ? intprec - maxprec : 0;
   PlaneResult pr;
-  if constexpr (N <= 64) pr = decode_planes_sync<N>(r, budget, kmin, intprec, ps);
+  if constexpr (N == 64) pr = decode_planes_sync<N, 0, true>(r, budget, kmin, intprec, ps);
+  else if constexpr (N < 64) pr = decode_planes_sync<N>(r, budget, kmin, intprec, ps);
   else pr = decode_planes<N>(r, budget, kmin, intprec, ps);
   h.low = pr.low;
   h.high = pr.high;
   h.z = pr.low == (int)intprec;
+  h.tail = pr.tail != 0;
+  h.tail_pos = pr.tail_pos;
   h.round = rounding == 2;
   h.m = pr.m;
   h.prec = pr.prec;
@@ -1997,16 +2060,66 @@ ZFPB_DEV u32 parse_ints(Reader& r, u32 maxbits, u32 maxprec, int rounding, Plane
   return pr.bits;
 }
 
+// 64-value blocks: planes [low, high] from the plane store and the verbatim
+// tail below them from the stream, then coefficients (as load_planes).  The
+// tail's last plane is k_last = intprec - prec (the reader's final k); it is
+// cut to m bits when m != 0, and the full planes are low - 1 .. k_last + 1
+// (or down to k_last when m == 0).
+template <class U>
+ZFPB_DEV void load_planes_tail(U* u, PlaneStore ps, const BlockHead& h, const TailSrc& ts) {
+  constexpr int P = sizeof(U) * 8;
+  const int lo = h.low, hi = h.high;
+  const int k_last = P - (int)h.prec;
+  const int tlo = !h.tail ? lo : (h.m != 0 ? k_last : k_last + 1);
+  const u64 w0 = h.tail_pos >> 6;
+  const u32 sh = (u32)(h.tail_pos & 63);
+  auto word = [&](u64 i) -> u64 { return i < ts.len ? __ldg(ts.stream + i) : 0ull; };
+  auto plane = [&](int k) -> u64 {
+    if (k >= lo && k <= hi) return ps.at(k, 0, 1);
+    if (k < tlo || k >= lo) return 0ull;
+    const u64 j = (u64)(lo - 1 - k);  // the tail's j-th plane
+    u64 v = word(w0 + j) >> sh;
+    if (sh) v |= word(w0 + j + 1) << (64 - sh);
+    if (h.m != 0 && k == k_last) v &= low_mask(h.m);
+    return v;
+  };
+  if constexpr (sizeof(U) == 4) {
+    u32 a[32], b[32];
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+      const u64 x = plane(k);
+      a[k] = (u32)x;
+      b[k] = (u32)(x >> 32);
+    }
+    transpose<u32, 32>(a);
+    transpose<u32, 32>(b);
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+      u[i] = a[i];
+      u[32 + i] = b[i];
+    }
+  } else {
+    u64 a[64];
+#pragma unroll
+    for (int k = 0; k < 64; k++) a[k] = plane(k);
+    transpose<u64, 64>(a);
+#pragma unroll
+    for (int i = 0; i < 64; i++) u[i] = a[i];
+  }
+}
+
 // decode_ints, value half: planes -> coefficients, inverse rounding, then the
 // inverse reorder and transform (decode/core.rs:97-131, KIND 1;
 // decode/reversible.rs:46-82, KIND 3).
 template <class I, int N, int KIND>
-ZFPB_DEV void finish_int_block(const BlockHead& h, I* ib, PlaneStore ps) {
+ZFPB_DEV void finish_int_block(const BlockHead& h, I* ib, PlaneStore ps, const TailSrc& ts) {
   typedef typename Traits<I>::U U;
   U u[N];
   if (h.z) {
 #pragma unroll
     for (int i = 0; i < N; i++) u[i] = 0;
+  } else if constexpr (N == 64) {
+    load_planes_tail<U>(u, ps, h, ts);
   } else {
     load_planes<U, N>(u, ps, h.low, h.high);
   }
@@ -2037,6 +2150,8 @@ ZFPB_DEV u32 parse_block(Reader& r, const Codec& c, PlaneStore ps, BlockHead& h,
   h.low = h.high = 0;
   h.m = h.prec = 0;
   h.round = h.z = false;
+  h.tail = false;
+  h.tail_pos = 0;
   u32 bits;
   if (c.minexp < ZFP_MIN_EXP) {
     if constexpr (!Traits<T>::FLOAT) {
@@ -2086,12 +2201,12 @@ ZFPB_DEV u32 parse_block(Reader& r, const Codec& c, PlaneStore ps, BlockHead& h,
 
 // Value half of decode_block.
 template <class T, int N>
-ZFPB_DEV void finish_block(const BlockHead& h, T* blk, PlaneStore ps) {
+ZFPB_DEV void finish_block(const BlockHead& h, T* blk, PlaneStore ps, const TailSrc& ts) {
   typedef typename Traits<T>::I I;
   typedef typename Traits<T>::U U;
   if constexpr (!Traits<T>::FLOAT) {
-    if (h.kind == HEAD_REV_INT) finish_int_block<I, N, 3>(h, reinterpret_cast<I*>(blk), ps);
-    else finish_int_block<I, N, 1>(h, reinterpret_cast<I*>(blk), ps);
+    if (h.kind == HEAD_REV_INT) finish_int_block<I, N, 3>(h, reinterpret_cast<I*>(blk), ps, ts);
+    else finish_int_block<I, N, 1>(h, reinterpret_cast<I*>(blk), ps, ts);
   } else {
     if (h.kind == HEAD_ZERO) {
 #pragma unroll
@@ -2100,10 +2215,10 @@ ZFPB_DEV void finish_block(const BlockHead& h, T* blk, PlaneStore ps) {
     }
     I ib[N];
     if (h.kind == HEAD_FLOAT) {
-      finish_int_block<I, N, 1>(h, ib, ps);
+      finish_int_block<I, N, 1>(h, ib, ps, ts);
       inv_cast<T, N>(ib, blk, h.emax);
     } else {
-      finish_int_block<I, N, 3>(h, ib, ps);
+      finish_int_block<I, N, 3>(h, ib, ps, ts);
       if (h.kind == HEAD_REV_REINTERP) {
         const U tc = (U)(~(U)0) >> 1;
 #pragma unroll
