@@ -345,7 +345,43 @@ ZFPB_DEV void inv_cast(const typename Traits<T>::I* ib, T* fb, int emax) {
 // is a[i], column c is bit c.
 // ---------------------------------------------------------------------------
 
+// The stages that move whole bytes (J = 32, 16, 8) are byte permutations of
+// each pair of rows: with rows (a, b) and J = 16, the new a takes the low
+// halves of a and b and the new b their high halves (J = 8: the even and the
+// odd bytes; J = 32: the low and high 32-bit words).  __byte_perm does one
+// 32-bit word of that in one instruction.
+ZFPB_DEV void bperm_pair(u32& a, u32& b, u32 sel_a, u32 sel_b) {
+  const u32 x = __byte_perm(a, b, sel_a), y = __byte_perm(a, b, sel_b);
+  a = x;
+  b = y;
+}
+template <int J> ZFPB_DEV void byte_stage_pair(u32& a, u32& b) {
+  if constexpr (J == 16) bperm_pair(a, b, 0x5410, 0x7632);
+  else bperm_pair(a, b, 0x6240, 0x7351);
+}
+template <int J> ZFPB_DEV void byte_stage_pair(u64& a, u64& b) {
+  u32 al = (u32)a, ah = (u32)(a >> 32), bl = (u32)b, bh = (u32)(b >> 32);
+  if constexpr (J == 32) {
+    a = (u64)al | ((u64)bl << 32);
+    b = (u64)ah | ((u64)bh << 32);
+  } else {
+    byte_stage_pair<J>(al, bl);
+    byte_stage_pair<J>(ah, bh);
+    a = (u64)al | ((u64)ah << 32);
+    b = (u64)bl | ((u64)bh << 32);
+  }
+}
+
 template <class W, int J> ZFPB_DEV void transpose_stage(W* a, int R) {
+  if constexpr (J >= 8) {
+#pragma unroll
+    for (int k = 0; k < 64; k += 2 * J) {
+      if (k >= R) break;
+#pragma unroll
+      for (int i = k; i < k + J; i++) byte_stage_pair<J>(a[i], a[i + J]);
+    }
+    return;
+  }
   W m;
   if constexpr (J == 32) m = (W)0x00000000ffffffffull;
   else if constexpr (J == 16) m = (W)0x0000ffff0000ffffull;
@@ -1001,7 +1037,7 @@ ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore
     bits -= empty;
     u32 k = intprec - empty;
     while (bits != 0 && k > kmin) {
-      if (N <= 16 && n == size) break;  // verbatim tail below
+      if (n == size) break;  // verbatim tail below
       k--;
       if constexpr (N == 4) {
         const u32 x = (u32)nibbles_at<QW>(q, 4 * (intprec - 1 - k)) & 15u;
@@ -1014,13 +1050,7 @@ ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore
         continue;
       }
       const u64 x = ps.at(k, 0, 1);
-      if (n == size) {
-        const u32 take = size < bits ? size : bits;
-        w.put(x & low_mask(take), take);
-        bits -= take;
-        continue;
-      }
-      const u64 y = x >> n;  // n < size <= 64
+      const u64 y = x >> n;  // n < size <= 64 (n == size leaves the loop)
       u64 glo = 0, ghi = 0;
       u32 glen = 1, nn = n;
       if (y != 0) {
@@ -1051,10 +1081,11 @@ ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore
       bits -= take;
       n = nn;
     }
-    if constexpr (N <= 16) {
+    {
       // Every coefficient significant: the remaining planes go out verbatim,
-      // 64 / size of them per write, cut at the budget.  After the loop above
-      // so that a warp's threads run it together.
+      // 64 / size of them per write (one for 64-value blocks), cut at the
+      // budget.  After the loop above so that a warp's threads run it
+      // together instead of alternating with the group-test planes.
       constexpr u32 per = 64 / size;
       while (bits != 0 && k > kmin) {
         u64 chunk = 0;
@@ -1082,10 +1113,6 @@ ZFPB_DEV u32 ctz64(u64 x) { return x ? (u32)__ffsll((long long)x) - 1 : 64u; }
 struct PlaneResult {
   u32 bits, m, prec;
   int low, high;  // stored planes are [low, high]; low = intprec if none
-  // With a verbatim tail left in the stream (decode_planes_sync's TAIL):
-  // whether one was found, and the stream bit where it starts.
-  u32 tail = 0;
-  u64 tail_pos = 0;
 };
 
 // decode_planes (bitplane.rs:675-790): planes go to the plane store.
@@ -1377,22 +1404,11 @@ ZFPB_DEV void group_tests(u64 t0, u64 t1, u32 n, u32 a, u32& end, u32& n_new, u3
 // Same contract and results as decode_planes, for N <= 64.  With QW != 0
 // (4-value blocks of QW * 16 planes) the planes go to the nibble string q
 // instead of the plane store.
-//
-// With TAIL (64-value blocks), the planes read once every coefficient is
-// significant are not stored: they are the stream's next bits verbatim, a
-// plane per 64 bits (the last one cut at the budget), so the reader's state
-// after them follows arithmetically and the value half reads them from the
-// stream itself.  The planes stored are then those down to the last group-test
-// plane (`low`), the tail planes run from low - 1 down, and the result's m
-// and prec are those of the full read.
-template <int N, int QW = 0, bool TAIL = false>
+template <int N, int QW = 0>
 ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 intprec, PlaneStore ps,
                                         u64* q = nullptr) {
   static_assert(N <= 64, "one plane word per plane");
   static_assert(QW == 0 || N == 4, "nibble planes are for 4-value blocks");
-  static_assert(!TAIL || N == 64, "verbatim tails are for 64-value blocks");
-  u32 tail = 0;
-  u64 tail_pos = 0;
   constexpr u32 size = N;
   // Plane kk (its bits and, with `np` planes, the ones below it) to the store.
   auto put = [&](u32 kk, u64 x, u32 np) {
@@ -1412,29 +1428,34 @@ ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 in
   bool done = false;
   while (bits != 0) {
     if (N <= 16 && n == size) break;  // verbatim tail below
-    if constexpr (TAIL) {
+    if constexpr (N == 64) {
       if (n == size) {
-        // Each remaining iteration reads a whole plane while more than a
+        // Every coefficient significant: the remaining planes are the
+        // stream's next bits verbatim, a plane per 64 bits while more than a
         // plane of budget is left (m = 0), then the rest of the budget as a
-        // last plane (m = those bits); or, out of planes, ends with m = 0
-        // and k one below kmin.
-        tail_pos = r.pos();
+        // last plane (m = those bits); out of planes, the read ends with
+        // m = 0 and k one below kmin.  One tight loop instead of the
+        // iterations above, so that a warp's threads run it together.
         const u32 full_left = (bits - 1) / size, planes_left = k - kmin;
         const u32 f = full_left < planes_left ? full_left : planes_left;
-        u32 used = f * size;
-        k -= f;
-        bits -= used;
+        for (u32 j = 0; j < f; j++) {
+          k--;
+          ps.at(k, 0, 1) = r.lo();
+          r.advance(size);
+        }
+        bits -= f * size;
+        if (f) low = (int)k;
+        m = 0;
         if (k <= kmin) {
-          m = 0;
           k = k - 1;
         } else {
-          k = k - 1;
+          k--;
+          ps.at(k, 0, 1) = r.lo() & low_mask(bits);
+          low = (int)k;
           m = bits;
-          used += bits;
+          r.advance(bits);
           bits = 0;
         }
-        tail = used != 0;
-        r.advance_far(used);
         done = true;
         break;
       }
@@ -1580,8 +1601,6 @@ ZFPB_DEV PlaneResult decode_planes_sync(Reader& rd, u32 budget, u32 kmin, u32 in
   res.prec = intprec - k;
   res.low = low;
   res.high = high;
-  res.tail = tail;
-  res.tail_pos = tail_pos;
   return res;
 }
 
@@ -1997,41 +2016,25 @@ struct BlockHead {
   u32 m, prec;    // inverse-rounding arguments
   bool round;     // ROUND_LAST
   bool z;         // no plane stored
-  // The planes below `low` left in the stream (64-value blocks): a verbatim
-  // run from bit tail_pos, one plane per 64 bits from plane low - 1 down,
-  // the last one cut to m bits when m != 0 (see decode_planes_sync).
-  bool tail;
-  u64 tail_pos;
 
-  // For 64-value blocks, in one word with the tail's offset from the block's
-  // first bit (`start`): kind 3 bits, emax + 2048 12, low 7, high + 1 7, m 7,
-  // prec 7, round, z, tail, tail offset 15 (a block has at most 16658 bits).
-  ZFPB_DEV u64 pack(u64 start) const {
-    const u64 toff = tail ? tail_pos - start : 0;
-    return (u64)kind | ((u64)(u32)(emax + 2048) & 0xfff) << 3 | (u64)((u32)low & 0x7f) << 15 |
-           (u64)((u32)(high + 1) & 0x7f) << 22 | (u64)(m & 0x7f) << 29 | (u64)(prec & 0x7f) << 36 |
-           (u64)round << 43 | (u64)z << 44 | (u64)tail << 45 | (toff & 0x7fff) << 46;
+  // kind 3 bits, emax + 2048 12 bits, low 9, high + 1 9, m 9, prec 8, round, z.
+  ZFPB_DEV u64 pack() const {
+    return (u64)kind | ((u64)(u32)(emax + 2048) & 0xfff) << 3 | (u64)((u32)low & 0x1ff) << 15 |
+           (u64)((u32)(high + 1) & 0x1ff) << 24 | (u64)(m & 0x1ff) << 33 | (u64)(prec & 0xff) << 42 |
+           (u64)round << 50 | (u64)z << 51;
   }
-  ZFPB_DEV static BlockHead unpack(u64 v, u64 start) {
+  ZFPB_DEV static BlockHead unpack(u64 v) {
     BlockHead h;
     h.kind = (u32)(v & 7);
     h.emax = (int)((v >> 3) & 0xfff) - 2048;
-    h.low = (int)((v >> 15) & 0x7f);
-    h.high = (int)((v >> 22) & 0x7f) - 1;
-    h.m = (u32)((v >> 29) & 0x7f);
-    h.prec = (u32)((v >> 36) & 0x7f);
-    h.round = (v >> 43) & 1;
-    h.z = (v >> 44) & 1;
-    h.tail = (v >> 45) & 1;
-    h.tail_pos = start + ((v >> 46) & 0x7fff);
+    h.low = (int)((v >> 15) & 0x1ff);
+    h.high = (int)((v >> 24) & 0x1ff) - 1;
+    h.m = (u32)((v >> 33) & 0x1ff);
+    h.prec = (u32)((v >> 42) & 0xff);
+    h.round = (v >> 50) & 1;
+    h.z = (v >> 51) & 1;
     return h;
   }
-};
-
-// Where the value half finds a block's verbatim tail: the stream (len words).
-struct TailSrc {
-  const u64* stream;
-  u64 len;
 };
 
 // decode_ints, stream half: read the planes into ps; returns bits read.
@@ -2042,14 +2045,11 @@ ZFPB_DEV u32 parse_ints(Reader& r, u32 maxbits, u32 maxprec, int rounding, Plane
   const u32 budget = constrained ? maxbits : 0xffffffffu;
   const u32 kmin = intprec > maxprec ? intprec - maxprec : 0;
   PlaneResult pr;
-  if constexpr (N == 64) pr = decode_planes_sync<N, 0, true>(r, budget, kmin, intprec, ps);
-  else if constexpr (N < 64) pr = decode_planes_sync<N>(r, budget, kmin, intprec, ps);
+  if constexpr (N <= 64) pr = decode_planes_sync<N>(r, budget, kmin, intprec, ps);
   else pr = decode_planes<N>(r, budget, kmin, intprec, ps);
   h.low = pr.low;
   h.high = pr.high;
   h.z = pr.low == (int)intprec;
-  h.tail = pr.tail != 0;
-  h.tail_pos = pr.tail_pos;
   h.round = rounding == 2;
   h.m = pr.m;
   h.prec = pr.prec;
@@ -2060,66 +2060,16 @@ ZFPB_DEV u32 parse_ints(Reader& r, u32 maxbits, u32 maxprec, int rounding, Plane
   return pr.bits;
 }
 
-// 64-value blocks: planes [low, high] from the plane store and the verbatim
-// tail below them from the stream, then coefficients (as load_planes).  The
-// tail's last plane is k_last = intprec - prec (the reader's final k); it is
-// cut to m bits when m != 0, and the full planes are low - 1 .. k_last + 1
-// (or down to k_last when m == 0).
-template <class U>
-ZFPB_DEV void load_planes_tail(U* u, PlaneStore ps, const BlockHead& h, const TailSrc& ts) {
-  constexpr int P = sizeof(U) * 8;
-  const int lo = h.low, hi = h.high;
-  const int k_last = P - (int)h.prec;
-  const int tlo = !h.tail ? lo : (h.m != 0 ? k_last : k_last + 1);
-  const u64 w0 = h.tail_pos >> 6;
-  const u32 sh = (u32)(h.tail_pos & 63);
-  auto word = [&](u64 i) -> u64 { return i < ts.len ? __ldg(ts.stream + i) : 0ull; };
-  auto plane = [&](int k) -> u64 {
-    if (k >= lo && k <= hi) return ps.at(k, 0, 1);
-    if (k < tlo || k >= lo) return 0ull;
-    const u64 j = (u64)(lo - 1 - k);  // the tail's j-th plane
-    u64 v = word(w0 + j) >> sh;
-    if (sh) v |= word(w0 + j + 1) << (64 - sh);
-    if (h.m != 0 && k == k_last) v &= low_mask(h.m);
-    return v;
-  };
-  if constexpr (sizeof(U) == 4) {
-    u32 a[32], b[32];
-#pragma unroll
-    for (int k = 0; k < 32; k++) {
-      const u64 x = plane(k);
-      a[k] = (u32)x;
-      b[k] = (u32)(x >> 32);
-    }
-    transpose<u32, 32>(a);
-    transpose<u32, 32>(b);
-#pragma unroll
-    for (int i = 0; i < 32; i++) {
-      u[i] = a[i];
-      u[32 + i] = b[i];
-    }
-  } else {
-    u64 a[64];
-#pragma unroll
-    for (int k = 0; k < 64; k++) a[k] = plane(k);
-    transpose<u64, 64>(a);
-#pragma unroll
-    for (int i = 0; i < 64; i++) u[i] = a[i];
-  }
-}
-
 // decode_ints, value half: planes -> coefficients, inverse rounding, then the
 // inverse reorder and transform (decode/core.rs:97-131, KIND 1;
 // decode/reversible.rs:46-82, KIND 3).
 template <class I, int N, int KIND>
-ZFPB_DEV void finish_int_block(const BlockHead& h, I* ib, PlaneStore ps, const TailSrc& ts) {
+ZFPB_DEV void finish_int_block(const BlockHead& h, I* ib, PlaneStore ps) {
   typedef typename Traits<I>::U U;
   U u[N];
   if (h.z) {
 #pragma unroll
     for (int i = 0; i < N; i++) u[i] = 0;
-  } else if constexpr (N == 64) {
-    load_planes_tail<U>(u, ps, h, ts);
   } else {
     load_planes<U, N>(u, ps, h.low, h.high);
   }
@@ -2150,8 +2100,6 @@ ZFPB_DEV u32 parse_block(Reader& r, const Codec& c, PlaneStore ps, BlockHead& h,
   h.low = h.high = 0;
   h.m = h.prec = 0;
   h.round = h.z = false;
-  h.tail = false;
-  h.tail_pos = 0;
   u32 bits;
   if (c.minexp < ZFP_MIN_EXP) {
     if constexpr (!Traits<T>::FLOAT) {
@@ -2201,12 +2149,12 @@ ZFPB_DEV u32 parse_block(Reader& r, const Codec& c, PlaneStore ps, BlockHead& h,
 
 // Value half of decode_block.
 template <class T, int N>
-ZFPB_DEV void finish_block(const BlockHead& h, T* blk, PlaneStore ps, const TailSrc& ts) {
+ZFPB_DEV void finish_block(const BlockHead& h, T* blk, PlaneStore ps) {
   typedef typename Traits<T>::I I;
   typedef typename Traits<T>::U U;
   if constexpr (!Traits<T>::FLOAT) {
-    if (h.kind == HEAD_REV_INT) finish_int_block<I, N, 3>(h, reinterpret_cast<I*>(blk), ps, ts);
-    else finish_int_block<I, N, 1>(h, reinterpret_cast<I*>(blk), ps, ts);
+    if (h.kind == HEAD_REV_INT) finish_int_block<I, N, 3>(h, reinterpret_cast<I*>(blk), ps);
+    else finish_int_block<I, N, 1>(h, reinterpret_cast<I*>(blk), ps);
   } else {
     if (h.kind == HEAD_ZERO) {
 #pragma unroll
@@ -2215,10 +2163,10 @@ ZFPB_DEV void finish_block(const BlockHead& h, T* blk, PlaneStore ps, const Tail
     }
     I ib[N];
     if (h.kind == HEAD_FLOAT) {
-      finish_int_block<I, N, 1>(h, ib, ps, ts);
+      finish_int_block<I, N, 1>(h, ib, ps);
       inv_cast<T, N>(ib, blk, h.emax);
     } else {
-      finish_int_block<I, N, 3>(h, ib, ps, ts);
+      finish_int_block<I, N, 3>(h, ib, ps);
       if (h.kind == HEAD_REV_REINTERP) {
         const U tc = (U)(~(U)0) >> 1;
 #pragma unroll

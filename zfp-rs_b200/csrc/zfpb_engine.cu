@@ -706,7 +706,7 @@ static cudaError_t decode_blocks(Workspace& ws, const Call& call, const DecodeAr
     const u64 planes = (call.type == 1 || call.type == 3) ? 32 : 64;
     if (stride < (1ull << 31) && ws.planes.ensure(planes * stride * sizeof(u64)) == cudaSuccess &&
         ws.heads.ensure(n * sizeof(u64)) == cudaSuccess) {
-      SplitArgs sa{(u64*)ws.planes.p, stride, (u64*)ws.heads.p, var ? 1 : 0};
+      SplitArgs sa{(u64*)ws.planes.p, stride, (u64*)ws.heads.p};
       cudaError_t e;
       {
         KernelTimer t(K_PARSE, s);

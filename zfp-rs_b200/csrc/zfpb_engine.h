@@ -96,13 +96,10 @@ struct DecodeArgs {
 };
 
 // Scratch of the two-kernel decoder: plane k of block i at planes[k * stride + i].
-// var: blocks start at their offsets (else at i * maxbits), which is where the
-// value half finds the verbatim tails the stream half leaves in the stream.
 struct SplitArgs {
   u64* planes;
   u64 stride;
   u64* heads;
-  int var;
 };
 
 // Whether two index tuples of the field can address the same element

@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(128, 8) k_parse(DecodeArgs a, SplitArgs sa) {
     return;
   }
   check_loads(pos, rb, occ, a.stream_len, a.flags);
-  sa.heads[blk] = h.pack(pos);
+  sa.heads[blk] = h.pack();
 }
 
 template <class T, int D>
@@ -397,10 +397,9 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_finish(Dec
   const u64 blk = (u64)blockIdx.x * blockDim.x + threadIdx.x;
   if (blk >= a.f.nblocks || (*(volatile unsigned*)a.flags & FLAG_BAD_INDEX)) return;
   PlaneStore ps{sa.planes + blk, (int)sa.stride};
-  const u64 pos = a.start + (sa.var ? a.offsets[blk] : blk * (u64)a.c.maxbits);
-  const BlockHead h = BlockHead::unpack(sa.heads[blk], pos);
+  const BlockHead h = BlockHead::unpack(sa.heads[blk]);
   T b[S::N];
-  finish_block<T, S::N>(h, b, ps, TailSrc{a.stream, a.stream_len});
+  finish_block<T, S::N>(h, b, ps);
   int len[4];
   i64 off = block_origin<D>(a.f, blk, len);
   scatter_block<T, D>(static_cast<T*>(a.data), a.f, off, len, b, a.owner, a.imin, blk);
@@ -639,7 +638,7 @@ __global__ void __launch_bounds__(128, 8) k_parse_batch(BatchArgs a) {
       continue;
     }
     check_loads(o0, rb, occ, it->stream_words, a.flags + t.item);
-    a.heads[col] = h.pack(o0);
+    a.heads[col] = h.pack();
   }
 }
 
@@ -652,10 +651,9 @@ __global__ void __launch_bounds__(128, KernelShape<T, 3>::MIN_CTAS) k_finish_bat
     const u64 blk = t.first + j;
     const u64 col = it->plane_base + blk;
     PlaneStore ps{a.planes + col, (int)a.plane_stride};
-    const u64 o0 = it->start + (it->fixed ? blk * (u64)it->c.maxbits : batch_offsets(a, it)[blk]);
-    const BlockHead h = BlockHead::unpack(a.heads[col], o0);
+    const BlockHead h = BlockHead::unpack(a.heads[col]);
     T b[64];
-    finish_block<T, 64>(h, b, ps, TailSrc{it->stream, it->stream_words});
+    finish_block<T, 64>(h, b, ps);
     int len[4];
     i64 off = block_origin<3>(it->f, blk, len);
     scatter_block<T, 3>(static_cast<T*>(it->data), it->f, off, len, b, nullptr, 0, blk);
