@@ -1008,25 +1008,25 @@ __device__ constexpr Plane4Tables kPlane4{};
 // coefficient it is implied and omitted with its marker.  This is bit for bit
 // what the reference's group-test loop writes, so the block's stream is the
 // concatenation of plane codes, cut at the budget.
+// Planes above the highest one-bit of any coefficient: top = that bit + 1.
+template <class U, int N> ZFPB_DEV u32 top_plane(const U* u) {
+  U all = 0;
+#pragma unroll
+  for (int i = 0; i < N; i++) all |= u[i];
+  if constexpr (sizeof(U) == 4) return 32 - __clz((int)all);
+  else return 64 - __clzll((long long)all);
+}
+
+// The plane loop of encode_ints for blocks of at most 64 values, from planes
+// already stored (ps; 4-value blocks: the nibble string q), top as above.
 template <class U, int N, class Wr>
-ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore ps) {
-  if constexpr (N > 64) {
-    return encode_ints_loop<U, N>(w, maxbits, maxprec, u, ps);
-  } else {
+ZFPB_DEV u32 encode_stored_planes(Wr& w, u32 maxbits, u32 maxprec, u32 top, PlaneStore ps, const u64* q) {
+  {
     constexpr u32 intprec = sizeof(U) * 8;
     constexpr u32 size = N;
     const u32 budget = with_maxbits(maxbits, maxprec, size) ? maxbits : 0xffffffffu;
     const u32 kmin = intprec > maxprec ? intprec - maxprec : 0;
-    U all = 0;
-#pragma unroll
-    for (int i = 0; i < N; i++) all |= u[i];
-    u32 top;
-    if constexpr (sizeof(U) == 4) top = 32 - __clz((int)all);
-    else top = 64 - __clzll((long long)all);
     constexpr int QW = N == 4 ? (int)intprec / 16 : 1;
-    u64 q[QW];
-    if constexpr (N == 4) store_nibbles<U>(u, q);
-    else store_planes<U, N>(u, ps);
 
     u32 bits = budget;
     u32 n = 0;
@@ -1105,6 +1105,20 @@ ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore
       }
     }
     return budget - bits;
+  }
+}
+
+template <class U, int N, class Wr>
+ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore ps) {
+  if constexpr (N > 64) {
+    return encode_ints_loop<U, N>(w, maxbits, maxprec, u, ps);
+  } else {
+    const u32 top = top_plane<U, N>(u);
+    constexpr int QW = N == 4 ? (int)sizeof(U) * 8 / 16 : 1;
+    u64 q[QW];
+    if constexpr (N == 4) store_nibbles<U>(u, q);
+    else store_planes<U, N>(u, ps);
+    return encode_stored_planes<U, N>(w, maxbits, maxprec, top, ps, q);
   }
 }
 
@@ -1678,6 +1692,75 @@ ZFPB_DEV u32 encode_float_block(Wr& w, const T* fb, const Codec& c, PlaneStore p
     fwd_cast<T, N>(ib, fb, emax);
     return hb + encode_int_block<I, N>(w, ib, sat_sub(c.minbits, hb), sat_sub(c.maxbits, hb), prec,
                                        c.rounding, ps);
+  }
+  w.put(0, 1);
+  if (c.minbits > 1) {
+    w.put_zeros(c.minbits - 1);
+    return c.minbits;
+  }
+  return 1;
+}
+
+// The same float block coder in two halves, so that one thread can prepare
+// a block (cast, transform, planes into the plane store) and another code it
+// from the store: a CTA orders its blocks by the expected length of their
+// sequential plane loop before coding them, so that the threads of a warp run
+// loops of similar length.
+struct BlockPrep {
+  u32 head;  // header value 2 * e + 1 (written in EBITS + 1 bits), 0: an empty block
+  u32 prec;  // precision of the integer coder
+  u32 top;   // one above the highest one-bit of any coefficient
+  u32 key;   // planes before the last coefficient turns significant
+};
+
+template <class T, int N>
+ZFPB_DEV BlockPrep prep_float_block(const T* fb, const Codec& c, PlaneStore ps) {
+  static_assert(N == 16 || N == 64, "plane-store blocks of one word per plane");
+  typedef typename Traits<T>::I I;
+  typedef typename Traits<T>::U U;
+  BlockPrep p;
+  const int emax = exponent_block<T, N>(fb);
+  const u32 prec = precision_f(emax, c.maxprec, c.minexp, Dims<N>::value, c.tight != 0);
+  const u32 e = prec != 0 ? (u32)(emax + Traits<T>::EBIAS) : 0u;
+  p.head = e != 0 ? 2 * e + 1 : 0u;
+  p.prec = prec;
+  p.top = 0;
+  p.key = 0;
+  if (e != 0) {
+    I ib[N];
+    fwd_cast<T, N>(ib, fb, emax);
+    fwd_axes<I, N, 0>(ib);
+    if (c.rounding == 1) fwd_round<I, N>(ib, prec);
+    U u[N];
+    fwd_order<N>(u, ib);
+    p.top = top_plane<U, N>(u);
+    store_planes<U, N>(u, ps);
+    // The group-test phase of the plane loop ends with the plane in which
+    // the last coefficient turns significant (its highest one-bit).
+    constexpr u32 intprec = sizeof(U) * 8;
+    const u32 kmin = intprec > prec ? intprec - prec : 0;
+    const u32 last = top_plane<U, 1>(u + N - 1);
+    const u32 stop = last > kmin + 1 ? last - 1 : kmin;
+    p.key = p.top > stop ? p.top - stop : 0u;
+  }
+  return p;
+}
+
+// encode/float.rs:22-113 from a prepared block (same bits as encode_float_block).
+template <class T, int N, class Wr>
+ZFPB_DEV u32 code_float_block(Wr& w, const BlockPrep& p, const Codec& c, PlaneStore ps) {
+  static_assert(N == 16 || N == 64, "plane-store blocks of one word per plane");
+  typedef typename Traits<T>::U U;
+  if (p.head != 0) {
+    constexpr u32 hb = Traits<T>::EBITS + 1;
+    w.put(p.head, hb);
+    u32 bits = encode_stored_planes<U, N>(w, sat_sub(c.maxbits, hb), p.prec, p.top, ps, nullptr);
+    const u32 mb = sat_sub(c.minbits, hb);
+    if (bits < mb) {
+      w.put_zeros(mb - bits);
+      bits = mb;
+    }
+    return hb + bits;
   }
   w.put(0, 1);
   if (c.minbits > 1) {

@@ -219,6 +219,69 @@ template <class T, int D> struct KernelShape {
 };
 
 // ---------------------------------------------------------------------------
+// Coding order inside a CTA.  The plane loop of a block runs one iteration per
+// plane until the last coefficient turns significant, a count that differs
+// from block to block (zero blocks: none; blocks with a spike: many), and a
+// warp runs as long as its longest block.  Lossy float blocks of 16 and 64
+// values are therefore prepared by their own thread (planes into the plane
+// store), ordered by that count across the CTA, and coded in that order, so
+// that the threads of a warp run loops of similar length.
+// ---------------------------------------------------------------------------
+template <class T, int D> struct SortedCoder {
+  static constexpr bool value = Traits<T>::FLOAT && (D == 2 || D == 3);
+};
+
+// Counting sort of the CTA's keys (clamped to 0..63; at most 256 threads,
+// every thread calls): returns the CTA-local index of the block this thread
+// codes.  Ends with a barrier.
+ZFPB_DEV int order_by_key(u32 key, u32* cnt, unsigned char* order) {
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 64; i += blockDim.x) cnt[i] = 0;
+  __syncthreads();
+  key = key < 63 ? key : 63;
+  const u32 rank = atomicAdd(&cnt[key], 1u);
+  __syncthreads();
+  if (tid < 32) {
+    const u32 c0 = cnt[2 * tid], c1 = cnt[2 * tid + 1];
+    u32 sum = c0 + c1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u32 v = __shfl_up_sync(0xffffffffu, sum, o);
+      if (tid >= o) sum += v;
+    }
+    const u32 ex = sum - c0 - c1;
+    cnt[2 * tid] = ex;
+    cnt[2 * tid + 1] = ex + c0;
+  }
+  __syncthreads();
+  order[cnt[key] + rank] = (unsigned char)tid;
+  __syncthreads();
+  return order[tid];
+}
+
+// Shared memory of the sorted coder (CTAs of at most 128 threads).
+struct SortSmem {
+  BlockPrep prep[128];
+  u32 cnt[64];
+  unsigned char order[128];
+};
+
+// Gather and prepare block `blk` (if in the field) into the plane store column
+// of this thread; returns its record.
+template <class T, int D>
+ZFPB_DEV BlockPrep prep_field_block(const void* data, const FieldGeom& f, const Codec& c, u64 blk, PlaneStore ps) {
+  BlockPrep p{0u, 0u, 0u, 0u};
+  if (blk < f.nblocks) {
+    int len[4];
+    const i64 off = block_origin<D>(f, blk, len);
+    T b[KernelShape<T, D>::N];
+    gather_block<T, D>(static_cast<const T*>(data), f, off, len, b);
+    p = prep_float_block<T, KernelShape<T, D>::N>(b, c, ps);
+  }
+  return p;
+}
+
+// ---------------------------------------------------------------------------
 // Fixed-size blocks (every block exactly maxbits bits): stage a CTA's bits in
 // shared memory, then store the stream words the CTA owns.  CTA j codes blocks
 // [jB, jB + B + X): the X extra blocks are the next CTA's first ones, which
@@ -243,7 +306,23 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_encode_fix
   __syncthreads();
 
   const u64 blk = first + tid;
-  if (blk < a.f.nblocks) {
+  bool sorted = false;
+  if constexpr (SortedCoder<T, D>::value) {
+    if (a.c.minexp >= ZFP_MIN_EXP) {
+      __shared__ SortSmem ss;
+      sorted = true;
+      const BlockPrep p = prep_field_block<T, D>(a.data, a.f, a.c, blk, ps);
+      ss.prep[tid] = p;
+      const int j = order_by_key(p.key, ss.cnt, ss.order);
+      if (first + j < a.f.nblocks) {
+        Writer<true> w;
+        w.init(stage, lb + (u64)j * maxbits, stage_words);
+        code_float_block<T, S::N>(w, ss.prep[j], a.c, PlaneStore{smem + j, nthr});
+        w.finish();
+      }
+    }
+  }
+  if (!sorted && blk < a.f.nblocks) {
     int len[4];
     i64 off = block_origin<D>(a.f, blk, len);
     T b[S::N];
@@ -276,7 +355,25 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_encode_var
   extern __shared__ u64 smem[];
   const int tid = threadIdx.x;
   PlaneStore ps{smem + tid, (int)blockDim.x};
-  const u64 blk = (u64)blockIdx.x * blockDim.x + tid;
+  const u64 base = (u64)blockIdx.x * blockDim.x;
+  const u64 blk = base + tid;
+  if constexpr (SortedCoder<T, D>::value) {
+    if (a.c.minexp >= ZFP_MIN_EXP) {
+      __shared__ SortSmem ss;
+      const BlockPrep p = prep_field_block<T, D>(a.data, a.f, a.c, blk, ps);
+      ss.prep[tid] = p;
+      const int j = order_by_key(p.key, ss.cnt, ss.order);
+      const u64 bj = base + j;
+      if (bj < a.f.nblocks) {
+        Writer<false> w;
+        w.init(a.slots + bj * a.slot_words, 0, a.slot_words);
+        const u32 bits = code_float_block<T, S::N>(w, ss.prep[j], a.c, PlaneStore{smem + j, (int)blockDim.x});
+        w.finish();
+        a.lengths[bj] = bits;
+      }
+      return;
+    }
+  }
   if (blk >= a.f.nblocks) return;
   int len[4];
   i64 off = block_origin<D>(a.f, blk, len);
