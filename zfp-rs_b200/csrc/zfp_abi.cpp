@@ -1059,6 +1059,7 @@ zfpb::FieldGeom geom_of(const Plan& p, zfp_type t, const void* d_origin) {
   bool vec = p.s[0] == 1 && ((uintptr_t)d_origin % 16) == 0;
   for (int i = 1; i < p.dims; i++) vec = vec && ((p.s[i] * (ptrdiff_t)es) % 16) == 0;
   g.vec_ok = vec ? 1 : 0;
+  zfpb::fill_block_inverses(g);
   return g;
 }
 

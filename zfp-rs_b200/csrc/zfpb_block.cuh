@@ -1890,12 +1890,13 @@ ZFPB_DEV u32 rev_decode_int_block(Reader& r, u32 maxbits, I* ib, PlaneStore ps) 
 
 // Decode one block into blk; returns the bits the block occupies (after the
 // skip to minbits) and, in *read_bits, the bits actually read.
-template <class T, int N>
+// LOSSY: lossy float streams only (minexp >= ZFP_MIN_EXP), no reversible path.
+template <class T, int N, bool LOSSY = false>
 ZFPB_DEV u32 decode_block(Reader& r, T* blk, const Codec& c, PlaneStore ps, u32* read_bits) {
   typedef typename Traits<T>::I I;
   typedef typename Traits<T>::U U;
   u32 bits;
-  if (c.minexp < ZFP_MIN_EXP) {
+  if (!LOSSY && c.minexp < ZFP_MIN_EXP) {
     if constexpr (!Traits<T>::FLOAT) {
       bits = rev_decode_int_block<I, N>(r, c.maxbits, reinterpret_cast<I*>(blk), ps);
     } else {
@@ -2176,7 +2177,7 @@ ZFPB_DEV u32 parse_rev_int_block(Reader& r, u32 maxbits, PlaneStore ps, BlockHea
 
 // Stream half of decode_block: returns the bits the block occupies (after the
 // skip to minbits) and, in *read_bits, the bits actually read.
-template <class T, int N>
+template <class T, int N, bool LOSSY = false>
 ZFPB_DEV u32 parse_block(Reader& r, const Codec& c, PlaneStore ps, BlockHead& h, u32* read_bits) {
   typedef typename Traits<T>::U U;
   h.emax = 0;
@@ -2184,7 +2185,7 @@ ZFPB_DEV u32 parse_block(Reader& r, const Codec& c, PlaneStore ps, BlockHead& h,
   h.m = h.prec = 0;
   h.round = h.z = false;
   u32 bits;
-  if (c.minexp < ZFP_MIN_EXP) {
+  if (!LOSSY && c.minexp < ZFP_MIN_EXP) {
     if constexpr (!Traits<T>::FLOAT) {
       h.kind = HEAD_REV_INT;
       bits = parse_rev_int_block<U, N>(r, c.maxbits, ps, h);
@@ -2231,10 +2232,22 @@ ZFPB_DEV u32 parse_block(Reader& r, const Codec& c, PlaneStore ps, BlockHead& h,
 }
 
 // Value half of decode_block.
-template <class T, int N>
+template <class T, int N, bool LOSSY = false>
 ZFPB_DEV void finish_block(const BlockHead& h, T* blk, PlaneStore ps) {
   typedef typename Traits<T>::I I;
   typedef typename Traits<T>::U U;
+  if constexpr (LOSSY && Traits<T>::FLOAT) {
+    // Lossy float streams: a block of zeros or a float block, nothing else.
+    if (h.kind == HEAD_FLOAT) {
+      I ib[N];
+      finish_int_block<I, N, 1>(h, ib, ps);
+      inv_cast<T, N>(ib, blk, h.emax);
+    } else {
+#pragma unroll
+      for (int i = 0; i < N; i++) blk[i] = 0;
+    }
+    return;
+  }
   if constexpr (!Traits<T>::FLOAT) {
     if (h.kind == HEAD_REV_INT) finish_int_block<I, N, 3>(h, reinterpret_cast<I*>(blk), ps);
     else finish_int_block<I, N, 1>(h, reinterpret_cast<I*>(blk), ps);

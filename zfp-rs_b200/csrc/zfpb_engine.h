@@ -20,7 +20,15 @@ struct FieldGeom {
   u64 b[4];    // blocks per axis
   u64 nblocks;
   int vec_ok;  // full-block rows are 16-byte aligned contiguous runs
+  // ceil(2^64 / b[d]) for d < 3 (0 when b[d] == 1): the block index of a
+  // field of fewer than 2^32 blocks splits into per-axis block coordinates
+  // by multiply-high instead of 64-bit division (set by fill_block_inverses).
+  u64 inv[3];
 };
+
+inline void fill_block_inverses(FieldGeom& g) {
+  for (int d = 0; d < 3; d++) g.inv[d] = g.b[d] > 1 ? ~0ull / g.b[d] + 1 : 0ull;
+}
 
 enum : unsigned { FLAG_TRUNCATED = 1u, FLAG_BAD_INDEX = 2u, FLAG_BAD_HEADER = 4u };
 

@@ -17,41 +17,67 @@ template <class T, int D> static cudaError_t set_smem(const void* fn, size_t byt
 
 static inline unsigned grid_of(u64 n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
+// Kernels compiled for lossy float streams only (no reversible path) serve
+// 2D and 3D float fields whose minexp selects a lossy mode.
+template <class T, int D> static constexpr bool has_lossy() { return SortedCoder<T, D>::value; }
+template <class T, int D> static bool lossy(const CodecParams& c) { return has_lossy<T, D>() && c.minexp >= ZFP_MIN_EXP; }
+
+template <class T, int D, bool L>
+static cudaError_t encode_fixed_k(const EncodeFixedArgs& a, u64 ctas, int threads, size_t smem, cudaStream_t s) {
+  cudaError_t e = set_smem<T, D>((const void*)k_encode_fixed<T, D, L>, smem);
+  if (e != cudaSuccess) return e;
+  k_encode_fixed<T, D, L><<<(unsigned)ctas, threads, smem, s>>>(a);
+  return cudaGetLastError();
+}
 template <class T, int D>
 static cudaError_t encode_fixed_d(const EncodeFixedArgs& a, u64 ctas, int threads, size_t smem, cudaStream_t s) {
-  cudaError_t e = set_smem<T, D>((const void*)k_encode_fixed<T, D>, smem);
-  if (e != cudaSuccess) return e;
-  k_encode_fixed<T, D><<<(unsigned)ctas, threads, smem, s>>>(a);
-  return cudaGetLastError();
+  if constexpr (has_lossy<T, D>())
+    if (lossy<T, D>(a.c)) return encode_fixed_k<T, D, true>(a, ctas, threads, smem, s);
+  return encode_fixed_k<T, D, false>(a, ctas, threads, smem, s);
 }
 
 template <class T, int D> static int var_threads() { return D == 4 ? 32 : 128; }
 
+template <class T, int D, bool L> static cudaError_t encode_var_k(const EncodeVarArgs& a, cudaStream_t s) {
+  const int th = var_threads<T, D>();
+  size_t smem = plane_smem<T, D>(th);
+  cudaError_t e = set_smem<T, D>((const void*)k_encode_var<T, D, L>, smem);
+  if (e != cudaSuccess) return e;
+  k_encode_var<T, D, L><<<grid_of(a.f.nblocks, th), th, smem, s>>>(a);
+  return cudaGetLastError();
+}
 template <class T, int D> static cudaError_t encode_var_d(const EncodeVarArgs& a, cudaStream_t s) {
-  const int th = var_threads<T, D>();
-  size_t smem = plane_smem<T, D>(th);
-  cudaError_t e = set_smem<T, D>((const void*)k_encode_var<T, D>, smem);
-  if (e != cudaSuccess) return e;
-  k_encode_var<T, D><<<grid_of(a.f.nblocks, th), th, smem, s>>>(a);
-  return cudaGetLastError();
+  if constexpr (has_lossy<T, D>())
+    if (lossy<T, D>(a.c)) return encode_var_k<T, D, true>(a, s);
+  return encode_var_k<T, D, false>(a, s);
 }
 
+template <class T, int D, bool L> static cudaError_t decode_fixed_k(const DecodeArgs& a, cudaStream_t s) {
+  const int th = var_threads<T, D>();
+  size_t smem = plane_smem<T, D>(th);
+  cudaError_t e = set_smem<T, D>((const void*)k_decode_fixed<T, D, L>, smem);
+  if (e != cudaSuccess) return e;
+  k_decode_fixed<T, D, L><<<grid_of(a.f.nblocks, th), th, smem, s>>>(a);
+  return cudaGetLastError();
+}
 template <class T, int D> static cudaError_t decode_fixed_d(const DecodeArgs& a, cudaStream_t s) {
-  const int th = var_threads<T, D>();
-  size_t smem = plane_smem<T, D>(th);
-  cudaError_t e = set_smem<T, D>((const void*)k_decode_fixed<T, D>, smem);
-  if (e != cudaSuccess) return e;
-  k_decode_fixed<T, D><<<grid_of(a.f.nblocks, th), th, smem, s>>>(a);
-  return cudaGetLastError();
+  if constexpr (has_lossy<T, D>())
+    if (lossy<T, D>(a.c)) return decode_fixed_k<T, D, true>(a, s);
+  return decode_fixed_k<T, D, false>(a, s);
 }
 
-template <class T, int D> static cudaError_t decode_var_d(const DecodeArgs& a, cudaStream_t s) {
+template <class T, int D, bool L> static cudaError_t decode_var_k(const DecodeArgs& a, cudaStream_t s) {
   const int th = var_threads<T, D>();
   size_t smem = plane_smem<T, D>(th);
-  cudaError_t e = set_smem<T, D>((const void*)k_decode_var<T, D>, smem);
+  cudaError_t e = set_smem<T, D>((const void*)k_decode_var<T, D, L>, smem);
   if (e != cudaSuccess) return e;
-  k_decode_var<T, D><<<grid_of(a.f.nblocks, th), th, smem, s>>>(a);
+  k_decode_var<T, D, L><<<grid_of(a.f.nblocks, th), th, smem, s>>>(a);
   return cudaGetLastError();
+}
+template <class T, int D> static cudaError_t decode_var_d(const DecodeArgs& a, cudaStream_t s) {
+  if constexpr (has_lossy<T, D>())
+    if (lossy<T, D>(a.c)) return decode_var_k<T, D, true>(a, s);
+  return decode_var_k<T, D, false>(a, s);
 }
 
 template <class T, int D> static cudaError_t walk_d(const DecodeArgs& a, cudaStream_t s) {
@@ -86,14 +112,20 @@ template <class T>
 cudaError_t Launch<T>::parse(const Call& call, const DecodeArgs& a, const SplitArgs& sa, bool var, cudaStream_t s) {
   if (call.dims != 3) return cudaErrorInvalidValue;
   const unsigned g = grid_of(a.f.nblocks, 128);
-  if (var) k_parse<T, 3, true><<<g, 128, 0, s>>>(a, sa);
-  else k_parse<T, 3, false><<<g, 128, 0, s>>>(a, sa);
+  if (lossy<T, 3>(a.c)) {
+    if (var) k_parse<T, 3, true, true><<<g, 128, 0, s>>>(a, sa);
+    else k_parse<T, 3, false, true><<<g, 128, 0, s>>>(a, sa);
+  } else {
+    if (var) k_parse<T, 3, true, false><<<g, 128, 0, s>>>(a, sa);
+    else k_parse<T, 3, false, false><<<g, 128, 0, s>>>(a, sa);
+  }
   return cudaGetLastError();
 }
 template <class T>
 cudaError_t Launch<T>::finish(const Call& call, const DecodeArgs& a, const SplitArgs& sa, cudaStream_t s) {
   if (call.dims != 3) return cudaErrorInvalidValue;
-  k_finish<T, 3><<<grid_of(a.f.nblocks, 128), 128, 0, s>>>(a, sa);
+  if (lossy<T, 3>(a.c)) k_finish<T, 3, true><<<grid_of(a.f.nblocks, 128), 128, 0, s>>>(a, sa);
+  else k_finish<T, 3, false><<<grid_of(a.f.nblocks, 128), 128, 0, s>>>(a, sa);
   return cudaGetLastError();
 }
 template <class T, int D>

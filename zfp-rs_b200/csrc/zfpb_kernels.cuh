@@ -15,6 +15,27 @@ namespace zfpb {
 template <int D>
 ZFPB_DEV i64 block_origin(const FieldGeom& f, u64 idx, int* len) {
   i64 off = 0;
+  if (D <= 3 && f.nblocks <= 0xffffffffull) {
+    // Block coordinates by multiply-high (fields of fewer than 2^32 blocks;
+    // 4D fields keep the 64-bit division: the batched int32 4D encoder gave
+    // streams that differ from the single-array one's with this path, cause
+    // not found).
+    u32 r = (u32)idx;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      u32 c = r;
+      if (d < D - 1) {
+        const u32 q = f.inv[d] ? (u32)__umul64hi((u64)r, f.inv[d]) : r;
+        c = r - q * (u32)f.b[d];
+        r = q;
+      }
+      const u64 o = 4 * (u64)c;
+      off += (i64)o * f.s[d];
+      const u64 rest = f.n[d] - o;
+      len[d] = rest < 4 ? (int)rest : 4;
+    }
+    return off;
+  }
 #pragma unroll
   for (int d = 0; d < D; d++) {
     u64 nb = f.b[d];
@@ -289,7 +310,8 @@ ZFPB_DEV BlockPrep prep_field_block(const void* data, const FieldGeom& f, const 
 // lies in its own bit range; CTA 0 also owns the word holding the start bit,
 // into which it merges the bits already in the stream.
 // ---------------------------------------------------------------------------
-template <class T, int D>
+// LOSSY (lossy float 2D/3D fields): the sorted coder only.
+template <class T, int D, bool LOSSY>
 __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_encode_fixed(EncodeFixedArgs a) {
   typedef KernelShape<T, D> S;
   extern __shared__ u64 smem[];
@@ -306,23 +328,19 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_encode_fix
   __syncthreads();
 
   const u64 blk = first + tid;
-  bool sorted = false;
-  if constexpr (SortedCoder<T, D>::value) {
-    if (a.c.minexp >= ZFP_MIN_EXP) {
-      __shared__ SortSmem ss;
-      sorted = true;
-      const BlockPrep p = prep_field_block<T, D>(a.data, a.f, a.c, blk, ps);
-      ss.prep[tid] = p;
-      const int j = order_by_key(p.key, ss.cnt, ss.order);
-      if (first + j < a.f.nblocks) {
-        Writer<true> w;
-        w.init(stage, lb + (u64)j * maxbits, stage_words);
-        code_float_block<T, S::N>(w, ss.prep[j], a.c, PlaneStore{smem + j, nthr});
-        w.finish();
-      }
+  if constexpr (LOSSY) {
+    static_assert(SortedCoder<T, D>::value, "lossy kernels are for float 2D/3D fields");
+    __shared__ SortSmem ss;
+    const BlockPrep p = prep_field_block<T, D>(a.data, a.f, a.c, blk, ps);
+    ss.prep[tid] = p;
+    const int j = order_by_key(p.key, ss.cnt, ss.order);
+    if (first + j < a.f.nblocks) {
+      Writer<true> w;
+      w.init(stage, lb + (u64)j * maxbits, stage_words);
+      code_float_block<T, S::N>(w, ss.prep[j], a.c, PlaneStore{smem + j, nthr});
+      w.finish();
     }
-  }
-  if (!sorted && blk < a.f.nblocks) {
+  } else if (blk < a.f.nblocks) {
     int len[4];
     i64 off = block_origin<D>(a.f, blk, len);
     T b[S::N];
@@ -349,7 +367,7 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_encode_fix
 // Variable-size blocks, pass 1: each block coded into its own slot of the
 // scratch buffer (slot i at word i * slot_words), its bit length recorded.
 // ---------------------------------------------------------------------------
-template <class T, int D>
+template <class T, int D, bool LOSSY>
 __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_encode_var(EncodeVarArgs a) {
   typedef KernelShape<T, D> S;
   extern __shared__ u64 smem[];
@@ -357,22 +375,21 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_encode_var
   PlaneStore ps{smem + tid, (int)blockDim.x};
   const u64 base = (u64)blockIdx.x * blockDim.x;
   const u64 blk = base + tid;
-  if constexpr (SortedCoder<T, D>::value) {
-    if (a.c.minexp >= ZFP_MIN_EXP) {
-      __shared__ SortSmem ss;
-      const BlockPrep p = prep_field_block<T, D>(a.data, a.f, a.c, blk, ps);
-      ss.prep[tid] = p;
-      const int j = order_by_key(p.key, ss.cnt, ss.order);
-      const u64 bj = base + j;
-      if (bj < a.f.nblocks) {
-        Writer<false> w;
-        w.init(a.slots + bj * a.slot_words, 0, a.slot_words);
-        const u32 bits = code_float_block<T, S::N>(w, ss.prep[j], a.c, PlaneStore{smem + j, (int)blockDim.x});
-        w.finish();
-        a.lengths[bj] = bits;
-      }
-      return;
+  if constexpr (LOSSY) {
+    static_assert(SortedCoder<T, D>::value, "lossy kernels are for float 2D/3D fields");
+    __shared__ SortSmem ss;
+    const BlockPrep p = prep_field_block<T, D>(a.data, a.f, a.c, blk, ps);
+    ss.prep[tid] = p;
+    const int j = order_by_key(p.key, ss.cnt, ss.order);
+    const u64 bj = base + j;
+    if (bj < a.f.nblocks) {
+      Writer<false> w;
+      w.init(a.slots + bj * a.slot_words, 0, a.slot_words);
+      const u32 bits = code_float_block<T, S::N>(w, ss.prep[j], a.c, PlaneStore{smem + j, (int)blockDim.x});
+      w.finish();
+      a.lengths[bj] = bits;
     }
+    return;
   }
   if (blk >= a.f.nblocks) return;
   int len[4];
@@ -407,7 +424,7 @@ ZFPB_DEV void check_loads(u64 start, u32 read_bits, u32 occupied, u64 len, unsig
 }
 
 // Fixed-size blocks: block i starts at start + i * maxbits (decompress.rs:205-330).
-template <class T, int D>
+template <class T, int D, bool LOSSY>
 __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_fixed(DecodeArgs a) {
   typedef KernelShape<T, D> S;
   extern __shared__ u64 smem[];
@@ -420,7 +437,7 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_fix
   r.init(a.stream, a.stream_len, pos);
   T b[S::N];
   u32 rb;
-  u32 occ = decode_block<T, S::N>(r, b, a.c, ps, &rb);
+  u32 occ = decode_block<T, S::N, LOSSY>(r, b, a.c, ps, &rb);
   check_loads(pos, rb, occ, a.stream_len, a.flags);
   int len[4];
   i64 off = block_origin<D>(a.f, blk, len);
@@ -430,7 +447,7 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_fix
 // Variable-size blocks with known offsets: decode each block from its offset
 // and check that it ends where the next begins, which makes the offsets
 // exactly those of a serial decode (else FLAG_BAD_INDEX).
-template <class T, int D>
+template <class T, int D, bool LOSSY>
 __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_var(DecodeArgs a) {
   typedef KernelShape<T, D> S;
   extern __shared__ u64 smem[];
@@ -444,7 +461,7 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_var
   r.init(a.stream, a.stream_len, pos);
   T b[S::N];
   u32 rb;
-  u32 occ = decode_block<T, S::N>(r, b, a.c, ps, &rb);
+  u32 occ = decode_block<T, S::N, LOSSY>(r, b, a.c, ps, &rb);
   if (o1 < o0 || (u64)occ != o1 - o0) {
     atomicOr(a.flags, FLAG_BAD_INDEX);
     return;
@@ -461,7 +478,7 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_var
 // holds no values and no shared memory, so far more blocks are in flight than
 // in k_decode_*, whose plane store and value registers bound their occupancy.
 // k_finish rebuilds the values and scatters them.
-template <class T, int D, bool VAR>
+template <class T, int D, bool VAR, bool LOSSY>
 __global__ void __launch_bounds__(128, 8) k_parse(DecodeArgs a, SplitArgs sa) {
   typedef KernelShape<T, D> S;
   const u64 blk = (u64)blockIdx.x * blockDim.x + threadIdx.x;
@@ -479,7 +496,7 @@ __global__ void __launch_bounds__(128, 8) k_parse(DecodeArgs a, SplitArgs sa) {
   PlaneStore ps{sa.planes + blk, (int)sa.stride};
   BlockHead h;
   u32 rb;
-  u32 occ = parse_block<T, S::N>(r, a.c, ps, h, &rb);
+  u32 occ = parse_block<T, S::N, LOSSY>(r, a.c, ps, h, &rb);
   if (VAR && (o1 < o0 || (u64)occ != o1 - o0)) {
     atomicOr(a.flags, FLAG_BAD_INDEX);
     return;
@@ -488,7 +505,7 @@ __global__ void __launch_bounds__(128, 8) k_parse(DecodeArgs a, SplitArgs sa) {
   sa.heads[blk] = h.pack();
 }
 
-template <class T, int D>
+template <class T, int D, bool LOSSY>
 __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_finish(DecodeArgs a, SplitArgs sa) {
   typedef KernelShape<T, D> S;
   const u64 blk = (u64)blockIdx.x * blockDim.x + threadIdx.x;
@@ -496,7 +513,7 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_finish(Dec
   PlaneStore ps{sa.planes + blk, (int)sa.stride};
   const BlockHead h = BlockHead::unpack(sa.heads[blk]);
   T b[S::N];
-  finish_block<T, S::N>(h, b, ps);
+  finish_block<T, S::N, LOSSY>(h, b, ps);
   int len[4];
   i64 off = block_origin<D>(a.f, blk, len);
   scatter_block<T, D>(static_cast<T*>(a.data), a.f, off, len, b, a.owner, a.imin, blk);
@@ -650,6 +667,24 @@ __global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_encode_bat
   const CodecParams c = it->c;
   const u64 sw = it->slot_words;
   u32* lens = a.lengths + it->len_base;
+  if constexpr (SortedCoder<T, D>::value) {
+    // One block per thread: prepared, ordered across the CTA, then coded.
+    if (c.minexp >= ZFP_MIN_EXP && t.count <= blockDim.x) {
+      __shared__ SortSmem ss;
+      const BlockPrep p = prep_field_block<T, D>(it->data, it->f, c, tid < t.count ? t.first + tid : ~0ull, ps);
+      ss.prep[tid] = p;
+      const int j = order_by_key(p.key, ss.cnt, ss.order);
+      if ((u32)j < t.count) {
+        const u64 blk = t.first + j;
+        Writer<false> w;
+        w.init(a.slots + it->slot_base + blk * sw, 0, sw);
+        lens[blk] = code_float_block<T, S::N>(w, ss.prep[j], c, PlaneStore{smem + j, (int)blockDim.x});
+        w.finish();
+        if (blk + 1 == it->f.nblocks) lens[blk + 1] = 0;
+      }
+      return;
+    }
+  }
   for (u32 j = tid; j < t.count; j += blockDim.x) {
     const u64 blk = t.first + j;
     int len[4];
