@@ -361,9 +361,14 @@ def main():
     call_ms = passes[dom] / calls
     achieved = algo / (call_ms / 1e3) / 1e9
     roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic_of(dom.split(" ")[0]),
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic_of(dom.split(" ")[0]) if n == 512 else None,
             "algorithmic_bytes_per_launch": algo, "avg_launch_ms": call_ms, "launches": calls,
             "other_pass_ms": {k: v / calls for k, v in passes.items() if k != dom}}
+    tr = roof["traffic"]
+    if tr and n == 512:
+        # profiles/traffic.json holds the measured DRAM bytes of a call at 384^3 scaled to 512^3
+        roof["traffic_over_algorithmic"] = tr / algo
+        roof["traffic_source"] = "ncu dram__bytes_{read,write}.sum on 384^3, scaled by (512/384)^3"
     launches = int(sum(v[1] for v in ktimes.values()) + 2 * ktimes["scan"][1])  # a scan is 3 kernels
 
     # End to end through the C ABI with pinned host buffers.
