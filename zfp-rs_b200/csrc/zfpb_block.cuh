@@ -520,6 +520,77 @@ template <class U, int N> ZFPB_DEV void load_planes(U* u, PlaneStore ps, int lo,
   }
 }
 
+// ---- narrow plane ranges of 64-bit blocks ----------------------------------
+//
+// A block of 64 coefficients of 64 bits codes only planes [kmin, top): those
+// below kmin = 64 - precision are dropped and none at or above top (one above
+// the highest one-bit) is set.  Fixed-precision streams of at most 32 planes
+// (and low-precision blocks of fixed-accuracy streams) span at most 32 planes,
+// so the 32-bit words u >> kmin hold every coded bit and two 32x32 transposes
+// give the planes: about a third of the 64x64 transpose's work, in 32-bit
+// instead of 64-bit operations.  The choice is made for a whole warp at once
+// (every thread of it narrow, else all wide), so the warp runs one transpose.
+
+// Planes kmin .. kmin + 31 (those below 64) of u, which has no bit at or
+// above kmin + 32.
+template <class U, int N> ZFPB_DEV void store_planes_narrow(const U* u, PlaneStore ps, u32 kmin) {
+  static_assert(sizeof(U) == 8 && N == 64, "64 coefficients of 64 bits");
+  u32 lo[32], hi[32];
+#pragma unroll
+  for (int i = 0; i < 32; i++) {
+    lo[i] = (u32)(u[i] >> kmin);
+    hi[i] = (u32)(u[32 + i] >> kmin);
+  }
+  transpose<u32, 32>(lo);
+  transpose<u32, 32>(hi);
+#pragma unroll
+  for (int j = 0; j < 32; j++)
+    if (kmin + j < 64) ps.at((int)kmin + j, 0, 1) = (u64)lo[j] | ((u64)hi[j] << 32);
+}
+
+// Bit planes of the coded range [kmin, top) into ps: the narrow form when
+// every thread of the warp allows it.
+template <class U, int N> ZFPB_DEV void store_coded_planes(const U* u, PlaneStore ps, u32 kmin, u32 top) {
+  if constexpr (sizeof(U) == 8 && N == 64) {
+    if (__all_sync(__activemask(), top <= kmin + 32)) {
+      store_planes_narrow<U, N>(u, ps, kmin);
+      return;
+    }
+  }
+  store_planes<U, N>(u, ps);
+}
+
+// Coefficients from the stored planes [lo, hi] (hi - lo < 32).
+template <class U, int N> ZFPB_DEV void load_planes_narrow(U* u, PlaneStore ps, int lo, int hi) {
+  static_assert(sizeof(U) == 8 && N == 64, "64 coefficients of 64 bits");
+  u32 a[32], b[32];
+#pragma unroll
+  for (int k = 0; k < 32; k++) {
+    const u64 x = lo + k <= hi ? ps.at(lo + k, 0, 1) : 0ull;
+    a[k] = (u32)x;
+    b[k] = (u32)(x >> 32);
+  }
+  transpose<u32, 32>(a);
+  transpose<u32, 32>(b);
+#pragma unroll
+  for (int i = 0; i < 32; i++) {
+    u[i] = (U)a[i] << lo;
+    u[32 + i] = (U)b[i] << lo;
+  }
+}
+
+// Coefficients from the stored planes [lo, hi] (planes outside it zero): the
+// narrow form when every thread of the warp allows it.
+template <class U, int N> ZFPB_DEV void load_coded_planes(U* u, PlaneStore ps, int lo, int hi) {
+  if constexpr (sizeof(U) == 8 && N == 64) {
+    if (__all_sync(__activemask(), hi - lo < 32)) {
+      load_planes_narrow<U, N>(u, ps, lo, hi);
+      return;
+    }
+  }
+  load_planes<U, N>(u, ps, lo, hi);
+}
+
 // ---- register planes of 4-value blocks ------------------------------------
 //
 // A 1D block's P = bits-of-U planes are 4 bits each, so all of them fit in
@@ -1115,9 +1186,10 @@ ZFPB_DEV u32 encode_ints(Wr& w, u32 maxbits, u32 maxprec, const U* u, PlaneStore
   } else {
     const u32 top = top_plane<U, N>(u);
     constexpr int QW = N == 4 ? (int)sizeof(U) * 8 / 16 : 1;
+    constexpr u32 intprec = sizeof(U) * 8;
     u64 q[QW];
     if constexpr (N == 4) store_nibbles<U>(u, q);
-    else store_planes<U, N>(u, ps);
+    else store_coded_planes<U, N>(u, ps, intprec > maxprec ? intprec - maxprec : 0, top);
     return encode_stored_planes<U, N>(w, maxbits, maxprec, top, ps, q);
   }
 }
@@ -1640,7 +1712,7 @@ ZFPB_DEV u32 decode_ints(Reader& r, u32 maxbits, u32 maxprec, int rounding, U* u
   } else if constexpr (QW != 0) {
     load_nibbles<U>(u, q);
   } else {
-    load_planes<U, N>(u, ps, pr.low, pr.high);
+    load_coded_planes<U, N>(u, ps, pr.low, pr.high);
   }
   bool round = rounding == 2;
   if (round) {
@@ -1734,11 +1806,11 @@ ZFPB_DEV BlockPrep prep_float_block(const T* fb, const Codec& c, PlaneStore ps) 
     U u[N];
     fwd_order<N>(u, ib);
     p.top = top_plane<U, N>(u);
-    store_planes<U, N>(u, ps);
-    // The group-test phase of the plane loop ends with the plane in which
-    // the last coefficient turns significant (its highest one-bit).
     constexpr u32 intprec = sizeof(U) * 8;
     const u32 kmin = intprec > prec ? intprec - prec : 0;
+    store_coded_planes<U, N>(u, ps, kmin, p.top);
+    // The group-test phase of the plane loop ends with the plane in which
+    // the last coefficient turns significant (its highest one-bit).
     const u32 last = top_plane<U, 1>(u + N - 1);
     const u32 stop = last > kmin + 1 ? last - 1 : kmin;
     p.key = p.top > stop ? p.top - stop : 0u;
@@ -2155,7 +2227,7 @@ ZFPB_DEV void finish_int_block(const BlockHead& h, I* ib, PlaneStore ps) {
 #pragma unroll
     for (int i = 0; i < N; i++) u[i] = 0;
   } else {
-    load_planes<U, N>(u, ps, h.low, h.high);
+    load_coded_planes<U, N>(u, ps, h.low, h.high);
   }
   if (h.round) inv_round<U, N>(u, h.m, h.prec);
   if (KIND == 1 && h.z && !h.round) {

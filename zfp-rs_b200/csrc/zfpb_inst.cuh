@@ -1,5 +1,5 @@
-// Kernel launchers for one scalar type; included once per type by
-// zfpb_inst_{i32,i64,f32,f64}.cu so the heavy templates compile in parallel.
+// Kernel launchers for one scalar type; included by zfpb_inst.cu, which the
+// Makefile compiles once per (type, group of passes) in parallel.
 #pragma once
 
 #include "zfpb_kernels.cuh"
