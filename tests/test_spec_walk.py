@@ -2,7 +2,7 @@
 
 The block offsets then come from the speculative parallel walk (segments
 walked from guessed starts, fixed up from the previous segment's exit); on
-fields large enough to give it several segments, the decoded values must be
+fields large enough to give it several segments (1-D to 4-D), the decoded values must be
 bit-identical to a decode with the compressor's index and to one whose
 offsets come from the serial one-thread walk (ZFPB_SERIAL_WALK=1), and a
 stream cut short must be reported as truncated either way.
@@ -44,6 +44,9 @@ CASES = [
     ((70, 66, 63), "float64", lambda: Z.ZfpConfig.fixed_accuracy(1e-6)),
     ((64, 64, 70), "float32", lambda: Z.ZfpConfig.fixed_precision(20)),
     ((50, 50, 50), "int64", lambda: Z.ZfpConfig.fixed_precision(40)),
+    ((24, 28, 32, 36), "float64", lambda: Z.ZfpConfig.fixed_accuracy(1e-6)),
+    ((36, 32, 28, 24), "float32", lambda: Z.ZfpConfig.fixed_precision(20).with_rounding("last")),
+    ((20, 24, 28, 40), "int32", lambda: Z.ZfpConfig.reversible()),
 ]
 
 

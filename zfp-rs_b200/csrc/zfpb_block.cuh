@@ -968,13 +968,16 @@ __device__ const unsigned short kOnesDoubled[256] = {
     0x3ffc, 0x7ffb, 0x7ffe, 0xffff};
 
 // The bits of y (at most N of them) with every one-bit doubled, as a
-// 128-bit value (lo, hi).
-template <int N> ZFPB_DEV void double_ones(u64 y, u64& lo, u64& hi) {
+// 128-bit value (lo, hi); hb is y's highest one-bit, so bytes past hb / 8
+// are zero and are skipped (a warp goes on while any of its threads has
+// bytes left).
+template <int N> ZFPB_DEV void double_ones(u64 y, u32 hb, u64& lo, u64& hi) {
   lo = 0;
   hi = 0;
   u32 r = 0;  // one-bits below the current byte
 #pragma unroll
   for (int i = 0; i < (N + 7) / 8; i++) {
+    if ((u32)i > (hb >> 3)) break;
     const u32 b = (u32)(y >> (8 * i)) & 0xffu;
     const u64 t = __ldg(kOnesDoubled + b);
     const u32 sh = 8 * i + r;  // at most 112
@@ -1128,7 +1131,7 @@ ZFPB_DEV u32 encode_stored_planes(Wr& w, u32 maxbits, u32 maxprec, u32 top, Plan
         const u32 hb = 63 - (u32)__clzll((long long)y);
         const u32 c = (u32)__popcll((long long)y);
         u64 elo, ehi;
-        double_ones<N>(y, elo, ehi);
+        double_ones<N>(y, hb, elo, ehi);
         const u32 p = hb + c;  // second copy of the highest one: written as 0
         if (p < 64) elo &= ~(1ull << p);
         else ehi &= ~(1ull << (p - 64));

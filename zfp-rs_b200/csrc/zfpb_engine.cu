@@ -743,12 +743,12 @@ __global__ void k_spec_write(SpecWalkArgs a, const SpecPiece* pieces, u64* off, 
 
 // Offsets (relative to start) of a variable-rate stream without an index by
 // the speculative parallel walk (k_spec_walk, k_spec_fix).  Sets *done when
-// a.offsets holds them; else (4D fields, short streams, a full list) the
-// caller walks serially.  ZFPB_SERIAL_WALK=1 turns it off.
+// a.offsets holds them; else (short streams, a full list) the caller walks
+// serially.  ZFPB_SERIAL_WALK=1 turns it off.
 static Status spec_walk(Workspace& ws, const Call& call, const DecodeArgs& a, cudaStream_t s, bool* done) {
   *done = false;
   const char* env = getenv("ZFPB_SERIAL_WALK");
-  if (call.dims > 3 || (env && env[0] == '1')) return OK;
+  if (env && env[0] == '1') return OK;
   const u64 n = call.f.nblocks;
   const u64 end_bits = a.stream_len * 64 > a.start ? a.stream_len * 64 - a.start : 0;
   if (n < 1024 || end_bits == 0) return OK;
@@ -758,6 +758,7 @@ static Status spec_walk(Workspace& ws, const Call& call, const DecodeArgs& a, cu
   // took to join the true walk: a few hundred bits for 1D (no lead-in), up
   // to a few thousand blocks for 2D and 3D (a lead-in of one segment; swept
   // at 0, 1, 2 and 4 segments on 2D f32 1024^2 and 3D f64 128^3 and 512^3).
+  // 4D fields take the 3D sizes.
   const u64 avg = std::max<u64>(1, end_bits / n);
   const u64 G = std::max<u64>(call.dims == 1 ? 128 : call.dims == 2 ? 256 : 512, n / 4096);
   const u64 L = call.dims == 1 ? 0 : G;

@@ -184,13 +184,15 @@ template <class T> cudaError_t Launch<T>::walk_batch(int dims, const BatchArgs& 
     default: return walk_batch_d<T, 4>(a, s);
   }
 }
-// One walker per warp: a CTA of 32 threads per segment.
+// One walker per warp: a CTA of 32 threads per segment (4-D: plus the
+// walker's plane store in dynamic shared memory).
 template <class T> cudaError_t Launch<T>::spec_walk(int dims, const SpecWalkArgs& a, cudaStream_t s) {
   const unsigned g = (unsigned)a.nseg;
   switch (dims) {
     case 1: k_spec_walk<T, 1><<<g, 32, 0, s>>>(a); break;
     case 2: k_spec_walk<T, 2><<<g, 32, 0, s>>>(a); break;
     case 3: k_spec_walk<T, 3><<<g, 32, 0, s>>>(a); break;
+    case 4: k_spec_walk<T, 4><<<g, 32, plane_smem<T, 4>(1), s>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
@@ -201,6 +203,7 @@ template <class T> cudaError_t Launch<T>::spec_fix(int dims, const SpecWalkArgs&
     case 1: k_spec_fix<T, 1><<<g, 32, 0, s>>>(a); break;
     case 2: k_spec_fix<T, 2><<<g, 32, 0, s>>>(a); break;
     case 3: k_spec_fix<T, 3><<<g, 32, 0, s>>>(a); break;
+    case 4: k_spec_fix<T, 4><<<g, 32, plane_smem<T, 4>(1), s>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
@@ -211,6 +214,7 @@ cudaError_t Launch<T>::spec_tail(int dims, const SpecWalkArgs& a, u64* off, u64 
     case 1: k_spec_tail<T, 1><<<1, 32, 0, s>>>(a, off, idx, n, x); break;
     case 2: k_spec_tail<T, 2><<<1, 32, 0, s>>>(a, off, idx, n, x); break;
     case 3: k_spec_tail<T, 3><<<1, 32, 0, s>>>(a, off, idx, n, x); break;
+    case 4: k_spec_tail<T, 4><<<1, 32, plane_smem<T, 4>(1), s>>>(a, off, idx, n, x); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -569,10 +569,21 @@ __global__ void __launch_bounds__(32) k_walk(DecodeArgs a) {
 // slower.
 // ---------------------------------------------------------------------------
 
+// The bits of the block at x.  4-D blocks (256 values) are measured by the
+// stream half of the decoder, as the serial walk does, with a one-thread
+// plane store in the CTA's dynamic shared memory (one walker per CTA).
 template <class T, int D> ZFPB_DEV u64 spec_len(const SpecWalkArgs& a, u64 x) {
   Reader r;
   r.init(a.stream, a.stream_len, a.start + x);
-  return block_length<T, KernelShape<T, D>::N>(r, a.c);
+  if constexpr (KernelShape<T, D>::N <= 64) {
+    return block_length<T, KernelShape<T, D>::N>(r, a.c);
+  } else {
+    extern __shared__ u64 smem[];
+    PlaneStore ps{smem, 1};
+    BlockHead h;
+    u32 rb;
+    return parse_block<T, KernelShape<T, D>::N>(r, a.c, ps, h, &rb);
+  }
 }
 
 ZFPB_DEV u64 seg_hi(const SpecWalkArgs& a, u64 sg) {
