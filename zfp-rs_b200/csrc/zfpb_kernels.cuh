@@ -243,6 +243,14 @@ template <class T, int D> struct KernelShape {
   // bytes of spills per thread): 512^3 float64 k_finish 0.727 -> 0.660 ms
   // (fixed-accuracy), 0.598 -> 0.538 ms (fixed-precision 32).
   static constexpr int FINISH_CTAS = sizeof(T) == 4 ? 4 : 2;
+  // Batch kernels of 1D and 2D blocks: a batch kernel also holds its tile's
+  // item (geometry, codec parameters, buffers) and loops over the tile's
+  // blocks, and left to itself the compiler gives it far more registers than
+  // the single-array kernel of the same codec (1D float encode 63 instead of
+  // 31, 2D float decode 112 instead of 63), halving the warps per SM.  These
+  // bounds hold them to the single-array kernels' budgets.
+  static constexpr int BATCH_ENC_CTAS = D == 1 ? 12 : D == 2 && sizeof(T) == 4 ? 5 : MIN_CTAS;
+  static constexpr int BATCH_DEC_CTAS = D == 1 ? 8 : D == 2 ? (sizeof(T) == 4 ? 8 : 4) : MIN_CTAS;
 };
 
 // ---------------------------------------------------------------------------
@@ -674,7 +682,7 @@ template <class T, int D> __global__ void k_spec_tail(SpecWalkArgs a, u64* off, 
 // ---------------------------------------------------------------------------
 
 template <class T, int D>
-__global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_encode_batch(BatchArgs a) {
+__global__ void __launch_bounds__(128, KernelShape<T, D>::BATCH_ENC_CTAS) k_encode_batch(BatchArgs a) {
   typedef KernelShape<T, D> S;
   extern __shared__ u64 smem[];
   const BatchTile t = a.tiles[blockIdx.x];
@@ -724,7 +732,7 @@ ZFPB_DEV const u64* batch_offsets(const BatchArgs& a, const BatchItem* it) {
 }
 
 template <class T, int D>
-__global__ void __launch_bounds__(128, KernelShape<T, D>::MIN_CTAS) k_decode_batch(BatchArgs a) {
+__global__ void __launch_bounds__(128, KernelShape<T, D>::BATCH_DEC_CTAS) k_decode_batch(BatchArgs a) {
   typedef KernelShape<T, D> S;
   extern __shared__ u64 smem[];
   const BatchTile t = a.tiles[blockIdx.x];
