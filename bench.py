@@ -392,19 +392,13 @@ def main():
     torch.cuda.empty_cache()
     oc = None if args.no_configs else configs_measure(Z, dev, args, peak)
 
-    # The serving loop, then the batched workload (2,000 mixed arrays) against
-    # one call per array.  Serving runs first: the batched workload's cached
-    # plans keep up to 8 GiB of round scratch each from the library's batch
-    # memory pool, and after them the serving lanes' scratch growth had to map
-    # new pool memory, stalling the serving worker ~30 ms at a time (p99
-    # 16-37 ms at 200-1,000 req/s against 1.3-1.5 ms in a process that serves
-    # first).
+    # Batched workload (2,000 mixed arrays) against one call per array.
+    bt = batched_measure(Z, dev, args) if args.batched_arrays > 0 else None
     rates = [float(r) for r in args.serve_rates.split(",") if r.strip()]
     sv = [serving_measure(Z, dev, args, r) for r in rates]
     if args.serve_small_rate > 0:
         sv.append(serving_measure(Z, dev, args, args.serve_small_rate, max_bytes=1 << 20))
     sv = sv or None
-    bt = batched_measure(Z, dev, args) if args.batched_arrays > 0 else None
 
     if rank == 0:
         line = {
