@@ -74,6 +74,9 @@ def parse():
                     help="skip the other workloads (64^3 latency, 8192^2 rates, int32 walk, int64 field)")
     ap.add_argument("--serve-small-rate", type=float, default=20000.0,
                     help="serving: rate of a stream of small requests (16 KB..1 MB); 0 skips")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="run only the serving legs and print their results as one JSON list (the main run "
+                         "starts this in a fresh process)")
     return ap.parse_args()
 
 
@@ -293,6 +296,9 @@ def main():
 
     Z = zfpb.load()
     L = Z.lib()
+    if args.serve_only:
+        print(json.dumps(serving_legs(Z, dev, args)))
+        return
     n = args.size
     field_np = host_field(n, seed=rank)
     field = torch.from_numpy(field_np).to(dev)
@@ -394,11 +400,7 @@ def main():
 
     # Batched workload (2,000 mixed arrays) against one call per array.
     bt = batched_measure(Z, dev, args) if args.batched_arrays > 0 else None
-    rates = [float(r) for r in args.serve_rates.split(",") if r.strip()]
-    sv = [serving_measure(Z, dev, args, r) for r in rates]
-    if args.serve_small_rate > 0:
-        sv.append(serving_measure(Z, dev, args, args.serve_small_rate, max_bytes=1 << 20))
-    sv = sv or None
+    sv = serving_in_child(args, local)
 
     if rank == 0:
         line = {
@@ -720,6 +722,37 @@ def serving_measure(Z, dev, args, rate, seed=7, max_bytes=256 << 20):
     del pool
     torch.cuda.empty_cache()
     return res
+
+
+def serving_legs(Z, dev, args):
+    """Every serving leg: the Poisson streams of --serve-rates, then the stream of small requests."""
+    rates = [float(r) for r in args.serve_rates.split(",") if r.strip()]
+    sv = [serving_measure(Z, dev, args, r) for r in rates]
+    if args.serve_small_rate > 0:
+        sv.append(serving_measure(Z, dev, args, args.serve_small_rate, max_bytes=1 << 20))
+    return sv
+
+
+def serving_in_child(args, local):
+    """The serving legs in a fresh process on this rank's GPU, as a serving
+    process runs.  Run inside this process after the other legs, the serving
+    loop's p99 latency at 200-1,000 req/s was 14-40 ms (mostly time queued
+    before launch) against 1.3-1.5 ms in a fresh process; the cause was not
+    found (not the loop's own launch, result collection or scratch growth,
+    timed inside the library), so the leg gets a process of its own."""
+    if not [r for r in args.serve_rates.split(",") if r.strip()] and args.serve_small_rate <= 0:
+        return None
+    cmd = [sys.executable, str(ROOT / "bench.py"), "--serve-only", "--serve-rates", args.serve_rates,
+           "--serve-seconds", str(args.serve_seconds), "--serve-small-rate", str(args.serve_small_rate)]
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK=str(local))
+    r = subprocess.run(cmd, env=env, capture_output=True, text=True)
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("[")]
+    if r.returncode != 0 or not lines:
+        raise RuntimeError(f"serving legs failed (exit {r.returncode}): {r.stderr[-2000:]}")
+    sv = json.loads(lines[-1])
+    for leg in sv:
+        leg["process"] = "a fresh process started for the serving legs"
+    return sv or None
 
 
 def traffic_of(kind):
