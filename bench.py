@@ -744,14 +744,17 @@ def serving_in_child(args, local):
         return None
     cmd = [sys.executable, str(ROOT / "bench.py"), "--serve-only", "--serve-rates", args.serve_rates,
            "--serve-seconds", str(args.serve_seconds), "--serve-small-rate", str(args.serve_small_rate)]
-    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK=str(local))
+    # Eager module loading, as a latency-sensitive server should run: with lazy
+    # loading (CUDA's default) a kernel's first launch in the process stalls
+    # the serving loop 25-36 ms.
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK=str(local), CUDA_MODULE_LOADING="EAGER")
     r = subprocess.run(cmd, env=env, capture_output=True, text=True)
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("[")]
     if r.returncode != 0 or not lines:
         raise RuntimeError(f"serving legs failed (exit {r.returncode}): {r.stderr[-2000:]}")
     sv = json.loads(lines[-1])
     for leg in sv:
-        leg["process"] = "a fresh process started for the serving legs"
+        leg["process"] = "a fresh process started for the serving legs, CUDA_MODULE_LOADING=EAGER"
     return sv or None
 
 
