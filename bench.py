@@ -197,6 +197,16 @@ def max_over_ranks(pg, value, device):
 MODES = {"accuracy_1e-6": (1, 16658, 64, -20), "precision_32": (1, 16658, 32, -1074)}
 
 
+def workload_config(n, ws):
+    """The `config` of both arms' lines: the workload itself (each arm states
+    separately how it covers it)."""
+    return {"workload": f"{n}^3 float64 smooth x1e3 + 10% zero blocks + 1% spikes; fixed-accuracy 1e-6 and "
+                        f"fixed-precision 32, rounding First/Last x tight rotating per step",
+            "passes_per_step": "2 modes x (compress + decompress) of 1 field",
+            "l2": f"inputs ({n ** 3 * 8 / 2 ** 30:.3g} GiB) {'larger' if n ** 3 * 8 > 126e6 else 'not larger'} "
+                  f"than the 126 MB L2", "parallelism": f"replicas x{ws}"}
+
+
 def cpu_steps(slab, threads, steps, first_step=0, gpu_streams=None):
     """Steps of the oracle (the CPU restatement of zfp-rs) on `slab`: per step,
     both modes with the step's rounding, compress (chunked over `threads`) then
@@ -271,9 +281,7 @@ def run_reference(args):
             "impl": "reference", "value": v, "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": el * 1e3 / max(1, args.steps), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{args.size}^3 float64 smooth x1e3 + 10% zero blocks + 1% spikes; "
-                                   f"fixed-accuracy 1e-6 and fixed-precision 32, rounding First/Last x tight "
-                                   f"rotating per step", "sampled": sample},
+            "config": workload_config(args.size, ws), "sample": sample,
             "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
             "reference_toolchain": {"cargo": probe_cargo()},
             "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -408,11 +416,7 @@ def main():
             "value": value, "unit": "GB/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{n}^3 float64 smooth x1e3 + 10% zero blocks + 1% spikes; fixed-accuracy 1e-6 and "
-                                   f"fixed-precision 32, rounding First/Last x tight rotating per step",
-                       "passes_per_step": "2 modes x (compress + decompress) of 1 field",
-                       "l2": "inputs (1 GiB) larger than L2", "parallelism": f"replicas x{ws}",
-                       "mean_stream_bytes": mean_stream},
+            "config": workload_config(n, ws), "mean_stream_bytes": mean_stream,
             "roofline": roof,
             "kernel_ms": {k: {"total_ms": v[0], "launches": v[1]} for k, v in kinds.items()},
             "gpu_launches": launches,
