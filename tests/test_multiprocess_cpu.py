@@ -60,3 +60,8 @@ def test_reference_arm_prints_one_line_from_rank_zero():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] == "port"
+    # The same workload config as the GPU arm's line (how the arm samples it
+    # is stated beside it).
+    import bench
+
+    assert d["config"] == bench.workload_config(32, 2) and "slab" in d["sample"]
