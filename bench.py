@@ -752,7 +752,8 @@ def serving_in_child(args, local):
     # loading (CUDA's default) a kernel's first launch in the process stalls
     # the serving loop 25-36 ms.
     env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK=str(local), CUDA_MODULE_LOADING="EAGER")
-    r = subprocess.run(cmd, env=env, capture_output=True, text=True)
+    limit = 600 + 30 * args.serve_seconds * (len(args.serve_rates.split(",")) + 1)
+    r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=limit)
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("[")]
     if r.returncode != 0 or not lines:
         raise RuntimeError(f"serving legs failed (exit {r.returncode}): {r.stderr[-2000:]}")
