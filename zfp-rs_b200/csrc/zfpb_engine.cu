@@ -756,12 +756,14 @@ static Status spec_walk(Workspace& ws, const Call& call, const DecodeArgs& a, cu
   // or fewer; a lead-in of L blocks before each.  A walk takes L + G steps
   // plus its garbage start, and a fix about as many as the walks it meets
   // took to join the true walk: a few hundred bits for 1D (no lead-in), up
-  // to a few thousand blocks for 2D and 3D (a lead-in of one segment; swept
-  // at 0, 1, 2 and 4 segments on 2D f32 1024^2 and 3D f64 128^3 and 512^3).
-  // 4D fields take the 3D sizes.
+  // to a few thousand blocks for 2D and 3D.  Swept on 2D f32 1024^2 and 3D
+  // f64 128^3 and 512^3: a lead-in of one segment for 2D; half a segment for
+  // 3D (512^3 f64 fixed-accuracy: 26.9 ms at one segment, 20.3 ms at half,
+  // 22.4 ms at a quarter; segments of 256 or 1024 blocks were slower).  4D
+  // fields take the 3D sizes.
   const u64 avg = std::max<u64>(1, end_bits / n);
   const u64 G = std::max<u64>(call.dims == 1 ? 128 : call.dims == 2 ? 256 : 512, n / 4096);
-  const u64 L = call.dims == 1 ? 0 : G;
+  const u64 L = call.dims == 1 ? 0 : call.dims == 2 ? G : G / 2;
   const u64 seg_bits = G * avg;
   if (seg_bits >= (1ull << 31)) return OK;
   const u64 nseg = (end_bits + seg_bits - 1) / seg_bits;
