@@ -753,10 +753,14 @@ def serving_in_child(args, local):
     # the serving loop 25-36 ms.
     env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK=str(local), CUDA_MODULE_LOADING="EAGER")
     limit = 600 + 30 * args.serve_seconds * (len(args.serve_rates.split(",")) + 1)
-    r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=limit)
+    try:
+        r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=limit)
+    except subprocess.TimeoutExpired:
+        return [{"error": f"serving legs did not finish within {limit:.0f} s"}]
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("[")]
     if r.returncode != 0 or not lines:
-        raise RuntimeError(f"serving legs failed (exit {r.returncode}): {r.stderr[-2000:]}")
+        # Reported in the line instead of failing the whole benchmark.
+        return [{"error": f"serving legs failed (exit {r.returncode}): {r.stderr[-1000:]}"}]
     sv = json.loads(lines[-1])
     for leg in sv:
         leg["process"] = "a fresh process started for the serving legs, CUDA_MODULE_LOADING=EAGER"
