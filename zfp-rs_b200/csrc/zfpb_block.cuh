@@ -552,7 +552,7 @@ template <class U, int N> ZFPB_DEV void store_planes_narrow(const U* u, PlaneSto
 // every thread of the warp allows it.
 template <class U, int N> ZFPB_DEV void store_coded_planes(const U* u, PlaneStore ps, u32 kmin, u32 top) {
   if constexpr (sizeof(U) == 8 && N == 64) {
-    if (__all_sync(__activemask(), top <= kmin + 32)) {
+    if (__all_sync(__activemask(), kmin < 64 && top <= kmin + 32)) {  // kmin 64: no plane coded
       store_planes_narrow<U, N>(u, ps, kmin);
       return;
     }
